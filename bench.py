@@ -1,0 +1,309 @@
+"""RS(32,32) encode throughput on B200 (the reference's headline shape).
+
+Workload: GF(2^8) ReedSolomon(32, 32) encode, 1 MiB shards of uniform random bytes
+(seeded, generated on the device), STRIPES stripes per step, all resident in HBM. A
+step is one batched launch over all stripes (the FFT route, bitsliced). Inputs (32 GiB
+of data per step at the default size) are far larger than L2, so no flush is needed.
+
+Metric: algorithmic GB/s = (k + m) * shard_bytes * stripes / step time (read k shards,
+write m parity shards per stripe), also as a fraction of measured HBM copy bandwidth.
+Alongside: the plain matrix kernel one stripe per launch, the end-to-end rate through
+the public host-pointer API from pinned host memory, and the CPU baseline (the oracle's
+multi-threaded restatement of the reference's GFNI FFT path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+K_DATA, M_PARITY = 32, 32
+SHARD = 1 << 20
+METRIC = "RS(32,32) encode GB/s & % HBM peak, batched+tuned vs plain, 1 B200 bit-exact"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--stripes", type=int, default=1024, help="stripes per step per GPU")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the FFT kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "fft_kk_kernel_32_rs32x32_1MiB.md")
+    if not os.path.exists(path):
+        return None, None
+    per_stripe = None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_stripe:"):
+            per_stripe = float(line.split(":")[1])
+    return per_stripe, path
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.samples = []
+        if self.proc is None:
+            return
+        time.sleep(0.2)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.samples.append(f)
+
+    def summary(self):
+        if not self.samples:
+            return None
+        sm = [float(f[1]) for f in self.samples if f[1].replace(".", "").isdigit()]
+        mx = [float(f[2]) for f in self.samples if f[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for f in self.samples for i in range(4) if f[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline(seconds, threads=None):
+    """The oracle's multi-threaded GFNI replay of the reference FFT program, one stripe
+    per thread, looped over a bounded sample for about `seconds`."""
+    from oracle import oracle as O
+
+    threads = threads or os.cpu_count()
+    n_stripes = max(threads, 16)
+    shard = SHARD
+    rng = np.random.default_rng(7)
+    stripes = rng.integers(0, 256, size=(n_stripes, K_DATA + M_PARITY, shard), dtype=np.uint8)
+    total_t, total_b, reps = 0.0, 0, 0
+    while total_t < seconds:
+        total_t += O.encode8_batch_mt(K_DATA, M_PARITY, stripes, threads)
+        total_b += n_stripes * (K_DATA + M_PARITY) * shard
+        reps += 1
+    sample = ("%d stripes x RS(32,32) x 1 MiB shards, %d passes (%.1f s), %s path, one stripe per thread"
+              % (n_stripes, reps, total_t, "GFNI/AVX-512" if O.cpu_has_gfni() else "scalar"))
+    return {"value": total_b / total_t / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": sample}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    steps = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(max(1.0, args.cpu_seconds / max(args.steps, 1)))
+        if i >= args.warmup:
+            steps.append(b["value"])
+        base = b
+    value = statistics.mean(steps)
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded uniform bytes)",
+        "config": {"workload": "RS(32,32) encode, 1 MiB shards", "shard_bytes": SHARD, "k": K_DATA,
+                   "m": M_PARITY},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": base["cores"], "kind": "port",
+                         "sample": base["sample"]},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world):
+    import torch
+
+    import __graft_entry__
+
+    rsb = __graft_entry__.load_package()
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+    S, L, k, m = args.stripes, SHARD, K_DATA, M_PARITY
+    g = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    data = torch.randint(0, 256, (S, k, L), dtype=torch.uint8, device="cuda", generator=g)
+    parity = torch.empty((S, m, L), dtype=torch.uint8, device="cuda")
+    rs = rsb.ReedSolomon(k, m)
+    stream = torch.cuda.current_stream().cuda_stream
+    bytes_per_step = S * (k + m) * L
+
+    def step():
+        rs.encode_batch_dev(data, parity, L, S, stream=stream)
+
+    # Self-check before timing: matrix-route verify of FFT-route parity on two stripes.
+    step()
+    torch.cuda.synchronize()
+    for s in (0, S - 1):
+        shards = [data[s, i] for i in range(k)] + [parity[s, j] for j in range(m)]
+        if not rs.verify_dev(shards, L, stream=stream):
+            raise RuntimeError("self-check failed: parity of stripe %d does not verify" % s)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches0 = rsb.kernel_launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with Clocks(dev) as clk:
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for i in range(args.steps):
+            ev[i][0].record()
+            step()
+            ev[i][1].record()
+        t1.record()
+        torch.cuda.synchronize()
+    launches = rsb.kernel_launch_count() - launches0
+    total_ms = t0.elapsed_time(t1)
+    kern_ms = [a.elapsed_time(b) for a, b in ev]
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = bytes_per_step * world / (ms_per_step * 1e-3) / 1e9
+
+    # Plain: the matrix kernel, one stripe per launch.
+    rs_plain = rsb.ReedSolomon(k, m)
+    rs_plain.set_route("matrix")
+    n_plain = min(S, 16)
+    for s in range(2):
+        rs_plain.encode_batch_dev(data[s], parity[s], L, 1, stream=stream)
+    torch.cuda.synchronize()
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record()
+    for s in range(n_plain):
+        rs_plain.encode_batch_dev(data[s], parity[s], L, 1, stream=stream)
+    p1.record()
+    torch.cuda.synchronize()
+    plain_gbs = n_plain * (k + m) * L / (p0.elapsed_time(p1) * 1e-3) / 1e9
+
+    # End to end through the host-pointer API from pinned memory: H2D data, encode,
+    # D2H parity inside the timed region.
+    S_e2e = min(S, 64)
+    h_data = torch.empty((S_e2e, k, L), dtype=torch.uint8, pin_memory=True)
+    h_par = torch.empty((S_e2e, m, L), dtype=torch.uint8, pin_memory=True)
+    h_data.copy_(data[:S_e2e].cpu())
+    e2e_times = []
+    for rep in range(3):
+        torch.cuda.synchronize()
+        t_start = time.perf_counter()
+        rs.encode_batch_host(h_data.numpy(), h_par.numpy(), L, S_e2e)
+        e2e_times.append(time.perf_counter() - t_start)
+    e2e_t = min(e2e_times[1:])
+    e2e_gbs = S_e2e * (k + m) * L / e2e_t / 1e9
+    if not torch.equal(h_par[0].cuda(), parity[0]) or not torch.equal(h_par[S_e2e - 1].cuda(), parity[S_e2e - 1]):
+        raise RuntimeError("end-to-end parity differs from the device-resident parity")
+
+    hbm, hbm_kind = peaks()
+    kern_avg = statistics.mean(kern_ms)
+    achieved = bytes_per_step / (kern_avg * 1e-3) / 1e9
+    traffic_per_stripe, traffic_src = profile_traffic()
+    traffic = traffic_per_stripe * S if traffic_per_stripe else None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded uniform bytes, generated on device)",
+            "config": {"workload": "RS(32,32) encode, 1 MiB shards, %d stripes per launch" % S,
+                       "k": k, "m": m, "shard_bytes": L, "stripes_per_step": S,
+                       "route": rs.encode_route(L), "l2": "inputs (%.0f GiB/step) larger than L2" % (S * k * L / 2**30),
+                       "parallelism": "replicas over stripe partitions" if world > 1 else "1 GPU"},
+            "frac_of_hbm": value / world / hbm,
+            "plain": {"value": plain_gbs, "unit": "GB/s", "route": "matrix kernel, one stripe per launch",
+                      "stripes": n_plain},
+            "batched_over_plain": (value / world) / plain_gbs,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "kernel": "fft_kk_kernel<32> (one launch per step)",
+                         "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % hbm_kind if hbm_kind == "measured"
+                         else "fallback 6.65 TB/s", "traffic_source": traffic_src},
+            "e2e": {"value": e2e_gbs, "unit": "GB/s", "h2d_bytes_per_step": S_e2e * k * L,
+                    "d2h_bytes_per_step": S_e2e * m * L,
+                    "path": "ReedSolomon.encode_batch_host (C ABI rs8_encode_batch) from pinned host memory"},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        if world == 1:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    rank = int(os.environ.get("RANK", 0))
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank)
+        else:
+            run_ours(args, rank, world)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,243 @@
+/*
+ * rs_b200 — B200-native Reed-Solomon encode/reconstruct behind a C ABI.
+ *
+ * Drop-in boundary for the tape-reed-solomon (spool-labs/reed-solomon 0.2.2) coder
+ * API. Each entry point below names the reference item it replaces (paths relative
+ * to the reference crate root). All arithmetic runs in hand-written sm_100a CUDA
+ * kernels; there is no CPU fallback: without a usable CUDA device every computing
+ * call returns RS_ERR_NO_DEVICE.
+ *
+ * Conventions
+ *  - Status 0 is success. 1..14 follow the reference `Error` enum in declaration
+ *    order (src/errors.rs:7-20). Values >= 100 are device/runtime errors.
+ *  - Host-pointer calls (no suffix) take host buffers like the reference's slices,
+ *    copy them to the device, run the kernels and copy results back before they
+ *    return. `_dev` calls take device pointers and a cudaStream_t (as void*), and
+ *    return once the work is enqueued.
+ *  - The caller owns every shard buffer; the library owns codec and decoder handles
+ *    and the device tables they hold. Handles are safe to share between threads.
+ *  - Shards of the GF((2^8)^2) coder use the split-plane wire: a shard of 2N bytes
+ *    holds the N low bytes then the N high bytes (src/reedsolomon16.rs:4-7).
+ */
+#ifndef RS_B200_H
+#define RS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ---- status codes: src/errors.rs:7-20 ---- */
+enum rs_status {
+  RS_OK = 0,
+  RS_TOO_FEW_SHARDS = 1,
+  RS_TOO_MANY_SHARDS = 2,
+  RS_TOO_FEW_DATA_SHARDS = 3,
+  RS_TOO_MANY_DATA_SHARDS = 4,
+  RS_TOO_FEW_PARITY_SHARDS = 5,
+  RS_TOO_MANY_PARITY_SHARDS = 6,
+  RS_TOO_FEW_BUFFER_SHARDS = 7,
+  RS_TOO_MANY_BUFFER_SHARDS = 8,
+  RS_INCORRECT_SHARD_SIZE = 9,
+  RS_TOO_FEW_SHARDS_PRESENT = 10,
+  RS_EMPTY_SHARD = 11,
+  RS_INVALID_SHARD_FLAGS = 12,
+  RS_INVALID_INDEX = 13,
+  RS_SINGULAR_MATRIX = 14,
+  RS_ERR_CUDA = 100,          /* a CUDA runtime call failed */
+  RS_ERR_ALLOC = 101,         /* host or device allocation failed */
+  RS_ERR_INVALID_ARGUMENT = 102, /* null handle/pointer or unsupported option */
+  RS_ERR_NO_DEVICE = 103,     /* no usable CUDA device */
+  RS_ERR_TIMEOUT = 104,       /* a bounded device wait gave up */
+  RS_ERR_LENGTH_MISMATCH = 105 /* gf8_mul_slice lengths differ (the reference panics) */
+};
+
+/* Message text for a status (src/errors.rs:24-41 for 1..14). Never NULL. */
+const char *rs_strerror(int status);
+/* ABI version, (major << 16) | minor. */
+uint32_t rs_abi_version(void);
+
+typedef struct rs8_codec rs8_t;
+typedef struct rs8_decoder rs8_dec_t;
+typedef struct rs16_codec rs16_t;
+typedef struct rs16_decoder rs16_dec_t;
+
+/* =========================== ReedSolomon (GF(2^8)) =========================== */
+
+/* ReedSolomon::new, src/reedsolomon.rs:166-196. k = 0 -> TooFewDataShards,
+ * m = 0 -> TooFewParityShards, k + m > 256 -> TooManyShards. Builds the systematic
+ * generator on the current CUDA device and keeps its tables resident there. */
+int rs8_new(size_t data_shards, size_t parity_shards, rs8_t **out);
+/* impl Clone for ReedSolomon, src/reedsolomon.rs:725-739 (copies the plan cache). */
+int rs8_clone(const rs8_t *codec, rs8_t **out);
+void rs8_free(rs8_t *codec);
+/* data_shard_count / parity_shard_count / total_shard_count, src/reedsolomon.rs:255-265 */
+size_t rs8_data_shard_count(const rs8_t *codec);
+size_t rs8_parity_shard_count(const rs8_t *codec);
+size_t rs8_total_shard_count(const rs8_t *codec);
+/* impl PartialEq for ReedSolomon, src/reedsolomon.rs:741-746: compares (k, m). */
+int rs8_equal(const rs8_t *a, const rs8_t *b);
+/* Generator rows k..n-1 (m x k bytes) as built on the device; row-major. */
+int rs8_parity_matrix(const rs8_t *codec, uint8_t *out, size_t out_len);
+
+/* ReedSolomon::encode, src/reedsolomon.rs:271-278. shards[0..k) data, [k..n) parity,
+ * all `len` bytes. n != k+m -> TooFew/TooManyShards; len 0 -> EmptyShard. */
+int rs8_encode(rs8_t *codec, uint8_t *const *shards, size_t n_shards, size_t len);
+/* ReedSolomon::encode_sep, src/reedsolomon.rs:284-309. Like the reference it does
+ * not reject len 0 (then it is a no-op). */
+int rs8_encode_sep(rs8_t *codec, const uint8_t *const *data, size_t n_data,
+                   uint8_t *const *parity, size_t n_parity, size_t len);
+/* ReedSolomon::encode_rows_into, src/reedsolomon.rs:667-697: data is k rows of
+ * row_len bytes back to back, parity m rows. Wrong sizes -> IncorrectShardSize;
+ * row_len 0 is a no-op. (encode_rows, :652, is the facade asserting the same.) */
+int rs8_encode_rows(rs8_t *codec, const uint8_t *data, size_t data_len, size_t row_len,
+                    uint8_t *parity, size_t parity_len);
+/* Many stripes of one shape from host memory (the batched form of encode_rows_into):
+ * stripe s reads k rows of row_len bytes at data + s*data_stride and writes m rows at
+ * parity + s*parity_stride. Copies to and from the device are pipelined with the
+ * kernels over chunks of stripes on three streams; pinned host buffers copy at full
+ * PCIe rate in both directions at once. Returns when the parity is in host memory. */
+int rs8_encode_batch(rs8_t *codec, const uint8_t *data, size_t data_stride, uint8_t *parity,
+                     size_t parity_stride, size_t n_stripes, size_t row_len);
+/* ReedSolomon::verify, src/reedsolomon.rs:430-463: *ok = 1 iff every parity shard
+ * matches the recomputed parity. */
+int rs8_verify(rs8_t *codec, const uint8_t *const *shards, size_t n_shards, size_t len,
+               int *ok);
+/* ReedSolomon::reconstruct / reconstruct_data, src/reedsolomon.rs:470-477,615-641.
+ * present[i] != 0 marks a valid shard; lens[i] is the length of buffer i (a present
+ * shard's length; an absent buffer must already have the shard length, as for the
+ * reference's `(T, bool)` shards). data_only leaves missing parity untouched. */
+int rs8_reconstruct(rs8_t *codec, uint8_t *const *shards, const size_t *lens,
+                    const uint8_t *present, size_t n_shards, int data_only);
+/* ReedSolomon::reconstruct_rows, src/reedsolomon.rs:514-535. */
+int rs8_reconstruct_rows(rs8_t *codec, uint8_t *rows, size_t rows_len, size_t row_len,
+                         const uint8_t *present, size_t n_present);
+/* ReedSolomon::prepare_decode, src/reedsolomon.rs:484-505 -> PreparedDecoder. */
+int rs8_prepare_decode(rs8_t *codec, const uint8_t *present, size_t n_present,
+                       rs8_dec_t **out);
+/* PreparedDecoder::{reconstruct, reconstruct_data}, src/reedsolomon.rs:760-797:
+ * a different presence pattern -> InvalidShardFlags. */
+int rs8_dec_reconstruct(rs8_dec_t *dec, uint8_t *const *shards, const size_t *lens,
+                        const uint8_t *present, size_t n_shards, int data_only);
+int rs8_dec_clone(const rs8_dec_t *dec, rs8_dec_t **out);
+void rs8_dec_free(rs8_dec_t *dec);
+/* ReedSolomon::encode_route, src/reedsolomon.rs:239-253 (bench/test introspection):
+ * "fft-bitsliced" or "matrix" for this shard length. Never NULL. */
+const char *rs8_encode_route(const rs8_t *codec, size_t len);
+/* Test/bench hook like the reference's encode_scalar/encode_forced
+ * (src/reedsolomon.rs:365-424): route 0 = automatic, 1 = matrix, 2 = bitsliced FFT
+ * (falls back to matrix where the shape has no FFT program). */
+int rs8_set_route(rs8_t *codec, int route);
+
+/* ---- device-resident variants (device pointers, enqueued on `stream`) ---- */
+int rs8_encode_dev(rs8_t *codec, uint8_t *const *d_shards, size_t n_shards, size_t len,
+                   void *stream);
+int rs8_encode_sep_dev(rs8_t *codec, const uint8_t *const *d_data, size_t n_data,
+                       uint8_t *const *d_parity, size_t n_parity, size_t len, void *stream);
+int rs8_encode_rows_dev(rs8_t *codec, const uint8_t *d_data, size_t row_len,
+                        uint8_t *d_parity, void *stream);
+/* Many stripes of one shape in one launch: stripe s reads k rows of row_len bytes at
+ * d_data + s*data_stride and writes m rows at d_parity + s*parity_stride. */
+int rs8_encode_batch_dev(rs8_t *codec, const uint8_t *d_data, size_t data_stride,
+                         uint8_t *d_parity, size_t parity_stride, size_t n_stripes,
+                         size_t row_len, void *stream);
+/* Recomputes parity and compares on the device; waits for the result. */
+int rs8_verify_dev(rs8_t *codec, const uint8_t *const *d_shards, size_t n_shards, size_t len,
+                   int *ok, void *stream);
+/* Reconstruct over device shard buffers (same checks as rs8_reconstruct). */
+int rs8_reconstruct_dev(rs8_t *codec, uint8_t *const *d_shards, const size_t *lens,
+                        const uint8_t *present, size_t n_shards, int data_only, void *stream);
+/* Many stripes of one shape, each with its own erasure pattern, in one launch.
+ * Stripe s is n contiguous rows of row_len bytes at d_rows + s*stripe_stride;
+ * present is n_stripes x n flags (host memory). Decode matrices for all patterns
+ * are built on the device. statuses (host, optional) gets a per-stripe status. */
+int rs8_reconstruct_batch_dev(rs8_t *codec, uint8_t *d_rows, size_t stripe_stride,
+                              size_t n_stripes, size_t row_len, const uint8_t *present,
+                              int data_only, int *statuses, void *stream);
+
+/* ========================= ReedSolomon16 (GF((2^8)^2)) ========================= */
+
+/* ReedSolomon16::new, src/reedsolomon16.rs:281-319 (k + m <= 65536). */
+int rs16_new(size_t data_shards, size_t parity_shards, rs16_t **out);
+int rs16_clone(const rs16_t *codec, rs16_t **out);
+void rs16_free(rs16_t *codec);
+size_t rs16_data_shard_count(const rs16_t *codec);
+size_t rs16_parity_shard_count(const rs16_t *codec);
+size_t rs16_total_shard_count(const rs16_t *codec);
+int rs16_equal(const rs16_t *a, const rs16_t *b);
+/* Generator rows k..n-1 (m x k tower symbols) as built; row-major. */
+int rs16_parity_matrix(const rs16_t *codec, uint16_t *out, size_t out_len);
+/* ReedSolomon16::encode, src/reedsolomon16.rs:412-419: even nonzero equal lengths. */
+int rs16_encode(rs16_t *codec, uint8_t *const *shards, size_t n_shards, size_t len);
+/* ReedSolomon16::encode_sep, src/reedsolomon16.rs:422-446. */
+int rs16_encode_sep(rs16_t *codec, const uint8_t *const *data, size_t n_data,
+                    uint8_t *const *parity, size_t n_parity, size_t len);
+/* ReedSolomon16::verify, src/reedsolomon16.rs:450-505. */
+int rs16_verify(rs16_t *codec, const uint8_t *const *shards, size_t n_shards, size_t len,
+                int *ok);
+/* ReedSolomon16::{reconstruct, reconstruct_data}, src/reedsolomon16.rs:508-515. */
+int rs16_reconstruct(rs16_t *codec, uint8_t *const *shards, const size_t *lens,
+                     const uint8_t *present, size_t n_shards, int data_only);
+/* ReedSolomon16::reconstruct_rows, src/reedsolomon16.rs:544-565 (even row_len). */
+int rs16_reconstruct_rows(rs16_t *codec, uint8_t *rows, size_t rows_len, size_t row_len,
+                          const uint8_t *present, size_t n_present);
+/* ReedSolomon16::prepare_decode -> PreparedDecoder16, src/reedsolomon16.rs:518-541,710-753 */
+int rs16_prepare_decode(rs16_t *codec, const uint8_t *present, size_t n_present,
+                        rs16_dec_t **out);
+int rs16_dec_reconstruct(rs16_dec_t *dec, uint8_t *const *shards, const size_t *lens,
+                         const uint8_t *present, size_t n_shards, int data_only);
+int rs16_dec_clone(const rs16_dec_t *dec, rs16_dec_t **out);
+void rs16_dec_free(rs16_dec_t *dec);
+/* ReedSolomon16::encode_route, src/reedsolomon16.rs:335-346: "matrix". */
+const char *rs16_encode_route(const rs16_t *codec);
+int rs16_encode_dev(rs16_t *codec, uint8_t *const *d_shards, size_t n_shards, size_t len,
+                    void *stream);
+/* Many stripes of one shape: stripe s reads k rows at d_data + s*data_stride and
+ * writes m rows at d_parity + s*parity_stride, rows of row_len (even) bytes. */
+int rs16_encode_batch_dev(rs16_t *codec, const uint8_t *d_data, size_t data_stride,
+                          uint8_t *d_parity, size_t parity_stride, size_t n_stripes,
+                          size_t row_len, void *stream);
+int rs16_reconstruct_dev(rs16_t *codec, uint8_t *const *d_shards, const size_t *lens,
+                         const uint8_t *present, size_t n_shards, int data_only,
+                         void *stream);
+
+/* ============================== gf slice kernels ============================== */
+
+/* gf::mul_slice / mul_slice_xor, src/gf/mod.rs:69-85: out[i] (^)= c * in[i] over
+ * GF(2^8). Differing lengths -> RS_ERR_LENGTH_MISMATCH (the reference panics). */
+int gf8_mul_slice(uint8_t *out, size_t out_len, const uint8_t *in, size_t in_len, uint8_t c,
+                  int xor_into);
+int gf8_mul_slice_dev(uint8_t *d_out, const uint8_t *d_in, size_t n, uint8_t c, int xor_into,
+                      void *stream);
+
+/* ============================ device / diagnostics ============================ */
+
+/* 0 when a CUDA device is usable, RS_ERR_NO_DEVICE otherwise. */
+int rs_device_check(void);
+/* Host-side construction (no device needed), for tests and offline tools.
+ * field 8 or 16. Parity rows k..k+m-1 of the systematic generator the reference
+ * builds as vandermonde(n,k) * inverse(top) (src/reedsolomon.rs:155-159), m x k
+ * row-major, as u16. */
+int rs_generator_rows(int field, size_t k, size_t m, uint16_t *out, size_t out_len);
+/* Decode rows of a presence pattern: one row per missing shard (data ascending,
+ * then parity ascending), mapping the first k present shards to it; the composed
+ * form of src/reedsolomon.rs:539-585 and :877-889. *n_rows receives the count. */
+int rs_decode_rows(int field, size_t k, size_t m, const uint8_t *present, uint16_t *out,
+                   size_t out_len, size_t *n_rows);
+/* Number of this library's kernel launches so far in this process. */
+uint64_t rs_kernel_launch_count(void);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif

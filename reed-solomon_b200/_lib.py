@@ -1,0 +1,99 @@
+"""ctypes binding of librsb200.so (the C ABI declared in include/rs_b200.h).
+
+The shared library is built in-tree by build_lib.py. There is no CPU fallback: if
+the library is missing, or no CUDA device is usable, calls raise.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librsb200.so")
+
+_sz = ctypes.c_size_t
+_vp = ctypes.c_void_p
+_int = ctypes.c_int
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_u16p = ctypes.POINTER(ctypes.c_uint16)
+_szp = ctypes.POINTER(ctypes.c_size_t)
+_intp = ctypes.POINTER(ctypes.c_int)
+_pp = ctypes.POINTER(ctypes.c_void_p)
+
+# name -> (restype, argtypes); every symbol include/rs_b200.h declares.
+SIGNATURES = {
+    "rs_strerror": (ctypes.c_char_p, [_int]),
+    "rs_abi_version": (ctypes.c_uint32, []),
+    "rs_device_check": (_int, []),
+    "rs_kernel_launch_count": (ctypes.c_uint64, []),
+    "rs_generator_rows": (_int, [_int, _sz, _sz, _u16p, _sz]),
+    "rs_decode_rows": (_int, [_int, _sz, _sz, _u8p, _u16p, _sz, _szp]),
+    "rs8_new": (_int, [_sz, _sz, _pp]),
+    "rs8_clone": (_int, [_vp, _pp]),
+    "rs8_free": (None, [_vp]),
+    "rs8_data_shard_count": (_sz, [_vp]),
+    "rs8_parity_shard_count": (_sz, [_vp]),
+    "rs8_total_shard_count": (_sz, [_vp]),
+    "rs8_equal": (_int, [_vp, _vp]),
+    "rs8_parity_matrix": (_int, [_vp, _u8p, _sz]),
+    "rs8_encode": (_int, [_vp, _pp, _sz, _sz]),
+    "rs8_encode_sep": (_int, [_vp, _pp, _sz, _pp, _sz, _sz]),
+    "rs8_encode_rows": (_int, [_vp, _vp, _sz, _sz, _vp, _sz]),
+    "rs8_encode_batch": (_int, [_vp, _vp, _sz, _vp, _sz, _sz, _sz]),
+    "rs8_verify": (_int, [_vp, _pp, _sz, _sz, _intp]),
+    "rs8_reconstruct": (_int, [_vp, _pp, _szp, _u8p, _sz, _int]),
+    "rs8_reconstruct_rows": (_int, [_vp, _vp, _sz, _sz, _u8p, _sz]),
+    "rs8_prepare_decode": (_int, [_vp, _u8p, _sz, _pp]),
+    "rs8_dec_reconstruct": (_int, [_vp, _pp, _szp, _u8p, _sz, _int]),
+    "rs8_dec_clone": (_int, [_vp, _pp]),
+    "rs8_dec_free": (None, [_vp]),
+    "rs8_encode_route": (ctypes.c_char_p, [_vp, _sz]),
+    "rs8_set_route": (_int, [_vp, _int]),
+    "rs8_encode_dev": (_int, [_vp, _pp, _sz, _sz, _vp]),
+    "rs8_encode_sep_dev": (_int, [_vp, _pp, _sz, _pp, _sz, _sz, _vp]),
+    "rs8_encode_rows_dev": (_int, [_vp, _vp, _sz, _vp, _vp]),
+    "rs8_encode_batch_dev": (_int, [_vp, _vp, _sz, _vp, _sz, _sz, _sz, _vp]),
+    "rs8_verify_dev": (_int, [_vp, _pp, _sz, _sz, _intp, _vp]),
+    "rs8_reconstruct_dev": (_int, [_vp, _pp, _szp, _u8p, _sz, _int, _vp]),
+    "rs8_reconstruct_batch_dev": (_int, [_vp, _vp, _sz, _sz, _sz, _u8p, _int, _intp, _vp]),
+    "rs16_new": (_int, [_sz, _sz, _pp]),
+    "rs16_clone": (_int, [_vp, _pp]),
+    "rs16_free": (None, [_vp]),
+    "rs16_data_shard_count": (_sz, [_vp]),
+    "rs16_parity_shard_count": (_sz, [_vp]),
+    "rs16_total_shard_count": (_sz, [_vp]),
+    "rs16_equal": (_int, [_vp, _vp]),
+    "rs16_parity_matrix": (_int, [_vp, _u16p, _sz]),
+    "rs16_encode": (_int, [_vp, _pp, _sz, _sz]),
+    "rs16_encode_sep": (_int, [_vp, _pp, _sz, _pp, _sz, _sz]),
+    "rs16_verify": (_int, [_vp, _pp, _sz, _sz, _intp]),
+    "rs16_reconstruct": (_int, [_vp, _pp, _szp, _u8p, _sz, _int]),
+    "rs16_reconstruct_rows": (_int, [_vp, _vp, _sz, _sz, _u8p, _sz]),
+    "rs16_prepare_decode": (_int, [_vp, _u8p, _sz, _pp]),
+    "rs16_dec_reconstruct": (_int, [_vp, _pp, _szp, _u8p, _sz, _int]),
+    "rs16_dec_clone": (_int, [_vp, _pp]),
+    "rs16_dec_free": (None, [_vp]),
+    "rs16_encode_route": (ctypes.c_char_p, [_vp]),
+    "rs16_encode_dev": (_int, [_vp, _pp, _sz, _sz, _vp]),
+    "rs16_encode_batch_dev": (_int, [_vp, _vp, _sz, _vp, _sz, _sz, _sz, _vp]),
+    "rs16_reconstruct_dev": (_int, [_vp, _pp, _szp, _u8p, _sz, _int, _vp]),
+    "gf8_mul_slice": (_int, [_vp, _sz, _vp, _sz, ctypes.c_uint8, _int]),
+    "gf8_mul_slice_dev": (_int, [_vp, _vp, _sz, ctypes.c_uint8, _int, _vp]),
+}
+
+_lib = None
+
+
+def load():
+    """Load librsb200.so, raising if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                "librsb200.so is not built (run reed-solomon_b200/build_lib.py); "
+                "there is no CPU fallback")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib

@@ -1,0 +1,399 @@
+// FFT-route encode kernels: the Lin-Chung-Han additive FFT of the reference's
+// generated programs (src/fft.rs, src/fft_programs.rs), bitsliced for CUDA cores.
+//
+// For a (K, K) shape with K a power of two the reference's encode program is an
+// inverse transform of the K data rows on the coset {0..K-1} (interpolation,
+// src/fft.rs:198-203) followed by a forward transform on the coset {K..2K-1}
+// (src/fft.rs:330-343); its outputs are the K parity rows in order.
+//
+// Bitslicing. A thread's 32 byte columns of one shard (8 words) are transposed into
+// 8 bit planes (32 bits each); the transpose is its own inverse, so the same network
+// turns parity planes back into bytes. Multiplying a register by a constant c is then
+// the GF(2) matrix of c applied to the planes: plane b of c*x is the XOR of planes b'
+// of x for which bit b of c*2^b' is set. With c known at compile time that is a short
+// fixed XOR network (about 18 three-input LOP3 operations per multiply-accumulate on
+// 32 columns), instead of a table lookup per byte.
+//
+// Lane pairs. K registers x 8 planes do not fit one thread for K = 32, so a lane pair
+// shares each 32-column group: lane h holds program registers 2j + h. At level l >= 1 a
+// butterfly pairs registers i and i + 2^l (same lane) and its constant
+// WHAT[l][beta ^ base] depends only on register bits above l, never on bit 0, so both
+// lanes run the same straight-line code with the same constants. Level 0 pairs 2j with
+// 2j + 1: the lanes swap the register with one shuffle per plane and each keeps its
+// own half of the butterfly.
+#pragma once
+
+#include <cstdint>
+#include <type_traits>
+#include <utility>
+
+#include "kernels_matrix.cuh"
+
+namespace rsb {
+
+namespace fftc {
+
+constexpr uint8_t xt(uint8_t v) { return (uint8_t)((v << 1) ^ ((v & 0x80) ? 0x1d : 0)); }
+
+constexpr uint8_t gmul(uint8_t a, uint8_t b) {
+  uint8_t r = 0;
+  for (int i = 0; i < 8; i++) {
+    if (b & 1) r ^= a;
+    a = xt(a);
+    b >>= 1;
+  }
+  return r;
+}
+
+struct What {
+  uint8_t v[8][256];
+};
+
+// Normalised subspace polynomials: W_0(x) = x, W_{j+1}(x) = W_j(x) (W_j(x) + W_j(2^j)),
+// each level scaled so that its value at 2^j is 1.
+constexpr What make_what() {
+  What w{};
+  uint8_t raw[8][256] = {};
+  for (int x = 0; x < 256; x++) raw[0][x] = (uint8_t)x;
+  for (int j = 0; j + 1 < 8; j++) {
+    uint8_t pivot = raw[j][1 << j];
+    for (int x = 0; x < 256; x++) raw[j + 1][x] = gmul(raw[j][x], (uint8_t)(raw[j][x] ^ pivot));
+  }
+  for (int j = 0; j < 8; j++) {
+    uint8_t pivot = raw[j][1 << j], inv = 0;
+    for (int c = 1; c < 256; c++)
+      if (gmul(pivot, (uint8_t)c) == 1) {
+        inv = (uint8_t)c;
+        break;
+      }
+    for (int x = 0; x < 256; x++) w.v[j][x] = gmul(raw[j][x], inv);
+  }
+  return w;
+}
+
+inline constexpr What kWhat = make_what();
+
+// Bit b of c * 2^bp: entry (b, bp) of the GF(2) matrix of multiply-by-c.
+constexpr bool mbit(uint8_t c, int b, int bp) { return (gmul(c, (uint8_t)(1u << bp)) >> b) & 1; }
+
+template <int B, int E, class F>
+__device__ __forceinline__ void static_for(F &&f) {
+  if constexpr (B < E) {
+    f(std::integral_constant<int, B>{});
+    static_for<B + 1, E>(f);
+  }
+}
+
+using Reg = uint32_t[8];
+
+// d ^= C * s
+template <uint8_t C>
+__device__ __forceinline__ void mul_acc(Reg &d, const Reg &s) {
+  static_for<0, 8>([&](auto b) {
+    uint32_t acc = d[b];
+    static_for<0, 8>([&](auto bp) {
+      if constexpr (mbit(C, decltype(b)::value, decltype(bp)::value)) acc ^= s[bp];
+    });
+    d[b] = acc;
+  });
+}
+
+// d = C * s
+template <uint8_t C>
+__device__ __forceinline__ void mul_set(Reg &d, const Reg &s) {
+  static_for<0, 8>([&](auto b) {
+    uint32_t acc = 0;
+    static_for<0, 8>([&](auto bp) {
+      if constexpr (mbit(C, decltype(b)::value, decltype(bp)::value)) acc ^= s[bp];
+    });
+    d[b] = acc;
+  });
+}
+
+__device__ __forceinline__ void xor_into(Reg &d, const Reg &s) {
+#pragma unroll
+  for (int b = 0; b < 8; b++) d[b] ^= s[b];
+}
+
+// lo/hi butterfly with constant C; inverse: hi ^= lo, lo ^= C*hi; forward: lo ^= C*hi,
+// hi ^= lo (src/fft.rs:262-283).
+template <uint8_t C, bool INV>
+__device__ __forceinline__ void butterfly(Reg &lo, Reg &hi) {
+  if constexpr (INV) xor_into(hi, lo);
+  if constexpr (C == 1)
+    xor_into(lo, hi);
+  else if constexpr (C != 0)
+    mul_acc<C>(lo, hi);
+  if constexpr (!INV) xor_into(hi, lo);
+}
+
+// Lane-local level L >= 1 of a K-point transform on coset BETA; r[j] is register 2j+h.
+template <int K, int L, int BETA, bool INV>
+__device__ __forceinline__ void level_local(Reg (&r)[K / 2]) {
+  constexpr int S = 1 << L;
+  static_for<0, K / 2>([&](auto jj) {
+    constexpr int j = decltype(jj)::value;
+    constexpr int i = 2 * j;
+    if constexpr (((i >> L) & 1) == 0) {
+      constexpr int base = i & ~(2 * S - 1);
+      constexpr uint8_t c = kWhat.v[L][BETA ^ base];
+      butterfly<c, INV>(r[j], r[j + S / 2]);
+    }
+  });
+}
+
+// Level 0 across the lane pair. hmask is 0 on lane 0 (even registers), ~0 on lane 1.
+template <int K, int BETA, bool INV>
+__device__ __forceinline__ void level0_pair(Reg (&r)[K / 2], uint32_t hmask) {
+  static_for<0, K / 2>([&](auto jj) {
+    constexpr int j = decltype(jj)::value;
+    constexpr uint8_t c = kWhat.v[0][BETA ^ (2 * j)];
+    Reg p;
+#pragma unroll
+    for (int b = 0; b < 8; b++) p[b] = __shfl_xor_sync(0xffffffffu, r[j][b], 1);
+    if constexpr (INV) {
+      // hi' = lo ^ hi; lo' = lo ^ c*hi'. Lane 0 owns lo, lane 1 owns hi.
+      Reg t, v;
+#pragma unroll
+      for (int b = 0; b < 8; b++) {
+        t[b] = r[j][b] ^ p[b];
+        v[b] = r[j][b];
+      }
+      if constexpr (c == 1)
+        xor_into(v, t);
+      else if constexpr (c != 0)
+        mul_acc<c>(v, t);
+#pragma unroll
+      for (int b = 0; b < 8; b++) r[j][b] = (t[b] & hmask) | (v[b] & ~hmask);
+    } else {
+      // lo' = lo ^ c*hi; hi' = hi ^ lo'. Lane 0: own ^ c*p; lane 1: own ^ p ^ c*own.
+      Reg z, u;
+#pragma unroll
+      for (int b = 0; b < 8; b++) z[b] = (r[j][b] & hmask) | (p[b] & ~hmask);
+      if constexpr (c == 1) {
+#pragma unroll
+        for (int b = 0; b < 8; b++) u[b] = z[b];
+      } else if constexpr (c != 0) {
+        mul_set<c>(u, z);
+      } else {
+#pragma unroll
+        for (int b = 0; b < 8; b++) u[b] = 0;
+      }
+#pragma unroll
+      for (int b = 0; b < 8; b++) r[j][b] ^= u[b] ^ (p[b] & hmask);
+    }
+  });
+}
+
+template <int K, int L, int BETA, bool INV>
+__device__ __forceinline__ void levels_up(Reg (&r)[K / 2]) {  // L .. log2(K)-1
+  if constexpr ((1 << L) < K) {
+    level_local<K, L, BETA, INV>(r);
+    levels_up<K, L + 1, BETA, INV>(r);
+  }
+}
+
+template <int K, int L, int BETA, bool INV>
+__device__ __forceinline__ void levels_down(Reg (&r)[K / 2]) {  // L .. 1
+  if constexpr (L >= 1) {
+    level_local<K, L, BETA, INV>(r);
+    levels_down<K, L - 1, BETA, INV>(r);
+  }
+}
+
+template <int K>
+constexpr int log2k() {
+  int l = 0;
+  while ((1 << l) < K) l++;
+  return l;
+}
+
+}  // namespace fftc
+
+// One step of the 8x8 bit transpose within each byte lane: swaps the high S-bit
+// half of every 2S-bit block of a with the low half of b. Shifts are written as
+// integer multiplies so they can issue on the FMA pipe beside the LOP3s.
+template <int S, uint32_t MLO>
+__device__ __forceinline__ void tswap(uint32_t &a, uint32_t &b) {
+  uint32_t bs = b * (1u << S);
+  uint32_t as = __umulhi(a, 1u << (32 - S));
+  uint32_t na = (a & MLO) | (bs & ~MLO);
+  uint32_t nb = (b & ~MLO) | (as & MLO);
+  a = na;
+  b = nb;
+}
+
+// 32 bytes (word i holds columns 4i..4i+3) <-> 8 bit planes (plane b, bit 8q+i holds
+// bit b of byte q of word i). An involution.
+__device__ __forceinline__ void bit_transpose(uint32_t (&w)[8]) {
+  tswap<4, 0x0F0F0F0Fu>(w[0], w[4]);
+  tswap<4, 0x0F0F0F0Fu>(w[1], w[5]);
+  tswap<4, 0x0F0F0F0Fu>(w[2], w[6]);
+  tswap<4, 0x0F0F0F0Fu>(w[3], w[7]);
+  tswap<2, 0x33333333u>(w[0], w[2]);
+  tswap<2, 0x33333333u>(w[1], w[3]);
+  tswap<2, 0x33333333u>(w[4], w[6]);
+  tswap<2, 0x33333333u>(w[5], w[7]);
+  tswap<1, 0x55555555u>(w[0], w[1]);
+  tswap<1, 0x55555555u>(w[2], w[3]);
+  tswap<1, 0x55555555u>(w[4], w[5]);
+  tswap<1, 0x55555555u>(w[6], w[7]);
+}
+
+__device__ __forceinline__ void load32(const uint8_t *p, uint64_t remain, uint32_t (&w)[8]) {
+  if (remain >= 32 && (((uintptr_t)p & 15u) == 0)) {
+    uint4 a = __ldg(reinterpret_cast<const uint4 *>(p));
+    uint4 b = __ldg(reinterpret_cast<const uint4 *>(p + 16));
+    w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+    w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i++) w[i] = 0;
+  int n = remain < 32 ? (int)remain : 32;
+  for (int t = 0; t < n; t++) w[t >> 2] |= (uint32_t)p[t] << (8 * (t & 3));
+}
+
+__device__ __forceinline__ void store32(uint8_t *p, uint64_t remain, const uint32_t (&w)[8]) {
+  if (remain >= 32 && (((uintptr_t)p & 15u) == 0)) {
+    *reinterpret_cast<uint4 *>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4 *>(p + 16) = make_uint4(w[4], w[5], w[6], w[7]);
+    return;
+  }
+  int n = remain < 32 ? (int)remain : 32;
+  for (int t = 0; t < n; t++) p[t] = (uint8_t)(w[t >> 2] >> (8 * (t & 3)));
+}
+
+struct FftArgs {
+  const uint8_t *in_base;
+  uint64_t in_row_stride, in_stripe_stride;
+  uint8_t *out_base;
+  uint64_t out_row_stride, out_stripe_stride;
+  uint64_t len;
+  uint32_t n_stripes;
+  uint32_t groups_per_stripe;  // 32-column groups per stripe
+};
+
+constexpr int kFftThreads = 128;
+
+// grid.x covers (stripes x groups) lane pairs; one lane pair per 32-column group.
+template <int K, bool PTRS>
+__global__ void __launch_bounds__(kFftThreads)
+    fft_kk_kernel(const FftArgs a, const __grid_constant__ PtrTableT<PTRS> pt) {
+  using namespace fftc;
+  const uint64_t pair = ((uint64_t)blockIdx.x * kFftThreads + threadIdx.x) >> 1;
+  const uint32_t h = threadIdx.x & 1;
+  const uint32_t hmask = h ? 0xffffffffu : 0u;
+  const uint64_t total = (uint64_t)a.n_stripes * a.groups_per_stripe;
+  // Pairs past the end still run (on zeros) so every shuffle sees the full warp.
+  const bool live = pair < total;
+  const uint32_t s = live ? (uint32_t)(pair / a.groups_per_stripe) : 0;
+  const uint64_t col = live ? (pair % a.groups_per_stripe) * 32 : 0;
+  const uint64_t remain = live ? a.len - col : 0;
+  Reg r[K / 2];
+#pragma unroll
+  for (int j = 0; j < K / 2; j++) {
+    const uint8_t *row;
+    if constexpr (PTRS)
+      row = pt.in[2 * j + h];
+    else
+      row = a.in_base + s * a.in_stripe_stride + (uint64_t)(2 * j + h) * a.in_row_stride;
+    uint32_t w[8];
+    load32(row + col, remain, w);
+    bit_transpose(w);
+#pragma unroll
+    for (int b = 0; b < 8; b++) r[j][b] = w[b];
+  }
+  constexpr int LG = log2k<K>();
+  // Interpolate: inverse transform on coset 0, levels 0 .. LG-1.
+  level0_pair<K, 0, true>(r, hmask);
+  levels_up<K, 1, 0, true>(r);
+  // Evaluate on coset K: forward transform, levels LG-1 .. 0.
+  levels_down<K, LG - 1, K, false>(r);
+  level0_pair<K, K, false>(r, hmask);
+  if (!live) return;
+#pragma unroll
+  for (int j = 0; j < K / 2; j++) {
+    uint8_t *row;
+    if constexpr (PTRS)
+      row = pt.out[2 * j + h];
+    else
+      row = a.out_base + s * a.out_stripe_stride + (uint64_t)(2 * j + h) * a.out_row_stride;
+    uint32_t w[8];
+#pragma unroll
+    for (int b = 0; b < 8; b++) w[b] = r[j][b];
+    bit_transpose(w);
+    store32(row + col, remain, w);
+  }
+}
+
+// Shapes with a bitsliced FFT kernel.
+struct FftShape {
+  int k, m;
+};
+
+inline const FftShape *find_fft_shape(size_t k, size_t m) {
+  static const FftShape shapes[] = {{2, 2}, {4, 4}, {8, 8}, {16, 16}, {32, 32}};
+  for (const FftShape &s : shapes)
+    if ((size_t)s.k == k && (size_t)s.m == m) return &s;
+  return nullptr;
+}
+
+template <int K, bool PTRS>
+inline cudaError_t launch_fft_k(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
+  uint64_t pairs = (uint64_t)a.n_stripes * a.groups_per_stripe;
+  uint64_t blocks = (pairs * 2 + kFftThreads - 1) / kFftThreads;
+  fft_kk_kernel<K, PTRS><<<(unsigned)blocks, kFftThreads, 0, st>>>(a, pt);
+  return cudaGetLastError();
+}
+
+template <bool PTRS>
+inline int launch_fft_any(const FftShape &sh, const FftArgs &a, const PtrTableT<PTRS> &pt,
+                          cudaStream_t st) {
+  if (a.len == 0 || a.n_stripes == 0) return RS_OK;
+  cudaError_t e;
+  switch (sh.k) {
+    case 2: e = launch_fft_k<2, PTRS>(a, pt, st); break;
+    case 4: e = launch_fft_k<4, PTRS>(a, pt, st); break;
+    case 8: e = launch_fft_k<8, PTRS>(a, pt, st); break;
+    case 16: e = launch_fft_k<16, PTRS>(a, pt, st); break;
+    case 32: e = launch_fft_k<32, PTRS>(a, pt, st); break;
+    default: return RS_ERR_INVALID_ARGUMENT;
+  }
+  g_launches++;
+  if (e != cudaSuccess) {
+    set_cuda_error(e, "fft_kk_kernel launch");
+    return RS_ERR_CUDA;
+  }
+  return RS_OK;
+}
+
+inline int launch_fft8(const FftShape &sh, const uint8_t *in_base, uint64_t in_row, uint64_t in_stripe,
+                       uint8_t *out_base, uint64_t out_row, uint64_t out_stripe, uint32_t n_stripes,
+                       uint64_t len, cudaStream_t st) {
+  FftArgs a{};
+  a.in_base = in_base;
+  a.in_row_stride = in_row;
+  a.in_stripe_stride = in_stripe;
+  a.out_base = out_base;
+  a.out_row_stride = out_row;
+  a.out_stripe_stride = out_stripe;
+  a.len = len;
+  a.n_stripes = n_stripes;
+  a.groups_per_stripe = (uint32_t)((len + 31) / 32);
+  PtrTableT<false> pt{};
+  return launch_fft_any<false>(sh, a, pt, st);
+}
+
+inline int launch_fft8_ptrs(const FftShape &sh, uint8_t *const *shards, uint64_t len, cudaStream_t st) {
+  FftArgs a{};
+  a.len = len;
+  a.n_stripes = 1;
+  a.groups_per_stripe = (uint32_t)((len + 31) / 32);
+  PtrTableT<true> pt;
+  for (int i = 0; i < sh.k; i++) pt.in[i] = shards[i];
+  for (int j = 0; j < sh.m; j++) pt.out[j] = shards[sh.k + j];
+  return launch_fft_any<true>(sh, a, pt, st);
+}
+
+}  // namespace rsb

@@ -1,0 +1,446 @@
+// C ABI of the ReedSolomon16 (GF((2^8)^2) tower) coder: include/rs_b200.h.
+// Split-plane wire: a shard of 2N bytes is N low bytes then N high bytes
+// (src/reedsolomon16.rs:4-7).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "runtime.hpp"
+#include "gf_host.hpp"
+#include "kernels_matrix.cuh"
+
+namespace rsb {
+
+// Karatsuba constants of a tower coefficient c = (c_hi, c_lo):
+// k0 = c_lo, k1 = c_hi ^ c_lo, k2 = c_hi * 32 (src/reedsolomon16.rs:61-94).
+static inline uint32_t split16(uint16_t c) {
+  uint8_t hi = c >> 8, lo = c & 0xff;
+  return (uint32_t)lo | ((uint32_t)(uint8_t)(hi ^ lo) << 8) | ((uint32_t)gf8_mul(hi, 32) << 16);
+}
+
+struct Gen16 {
+  int device = 0;
+  size_t k = 0, m = 0;
+  std::vector<uint16_t> rows;  // m x k
+  uint32_t *d_split = nullptr;
+  ~Gen16() {
+    if (d_split) {
+      cudaSetDevice(device);
+      cudaFree(d_split);
+    }
+  }
+};
+
+static int upload_split(const std::vector<uint16_t> &rows, uint32_t **out) {
+  std::vector<uint32_t> split(rows.size());
+  for (size_t t = 0; t < rows.size(); t++) split[t] = split16(rows[t]);
+  RSB_CU(cudaMalloc(out, std::max<size_t>(split.size(), 1) * 4));
+  RSB_CU(cudaMemcpy(*out, split.data(), split.size() * 4, cudaMemcpyHostToDevice));
+  return RS_OK;
+}
+
+static int launch_gf16(const Apply16Args &a, bool verify, cudaStream_t st) {
+  if (a.n_sym == 0 || a.rows == 0 || a.n_stripes == 0) return RS_OK;
+  uint64_t tiles = (a.n_sym + kThreads * 8 - 1) / (kThreads * 8);
+  dim3 grid((unsigned)tiles, std::min<uint32_t>(a.n_stripes, 65535), (a.rows + kRowChunk16 - 1) / kRowChunk16);
+  if (verify)
+    gf16_matrix_kernel<4, true><<<grid, kThreads, 0, st>>>(a);
+  else
+    gf16_matrix_kernel<4, false><<<grid, kThreads, 0, st>>>(a);
+  g_launches++;
+  RSB_CU(cudaGetLastError());
+  return RS_OK;
+}
+
+// Shard-length rule of the tower coder, src/reedsolomon16.rs:758-772.
+static int check_len16(size_t len) {
+  if (len == 0) return RS_EMPTY_SHARD;
+  if (len % 2) return RS_INCORRECT_SHARD_SIZE;
+  return RS_OK;
+}
+
+}  // namespace rsb
+
+using namespace rsb;
+
+struct rs16_codec {
+  std::shared_ptr<const Gen16> gen;
+  std::shared_ptr<PlanCache> plans;
+  std::shared_ptr<Exec> exec;
+};
+
+struct rs16_decoder {
+  std::shared_ptr<const Gen16> gen;
+  std::shared_ptr<const Plan> plan;
+  std::shared_ptr<Exec> exec;
+};
+
+namespace rsb {
+
+// Plan of one presence pattern: closed-form Lagrange rows from the survivors to each
+// missing shard (data ascending, then parity ascending), built on the host.
+static int plan16_for(const Gen16 &g, PlanCache &cache, const Presence &pres,
+                      std::shared_ptr<const Plan> &out) {
+  out = cache.find(pres);
+  if (out) return RS_OK;
+  auto plan = std::make_shared<Plan>();
+  plan->presence = pres;
+  plan->device = g.device;
+  split_pattern(pres, g.k, g.k + g.m, plan->survivors, plan->missing_data, plan->missing_parity);
+  if (plan->survivors.size() < g.k) return RS_TOO_FEW_SHARDS_PRESENT;
+  std::vector<size_t> nodes(plan->survivors.begin(), plan->survivors.end());
+  std::vector<size_t> targets(plan->missing_data.begin(), plan->missing_data.end());
+  targets.insert(targets.end(), plan->missing_parity.begin(), plan->missing_parity.end());
+  std::vector<uint16_t> rows;
+  lagrange_rows<F16>(nodes, targets, rows);
+  RSB_CU(cudaSetDevice(g.device));
+  uint32_t *d = nullptr;
+  RSB_TRY(upload_split(rows, &d));
+  plan->d_rows = d;
+  out = cache.insert(pres, plan);
+  return RS_OK;
+}
+
+// Runs out = rows x in over device rows; `in_ptrs`/`out_ptrs` are host arrays of
+// device pointers, copied into a stream-ordered device table.
+static int apply16_ptrs(const uint32_t *coeffs, uint32_t k, uint32_t rows, const uint8_t *const *in_ptrs,
+                        uint8_t *const *out_ptrs, size_t len, bool verify, uint32_t *mismatch,
+                        cudaStream_t st) {
+  std::vector<const uint8_t *> table(k + rows);
+  for (uint32_t i = 0; i < k; i++) table[i] = in_ptrs[i];
+  for (uint32_t j = 0; j < rows; j++) table[k + j] = out_ptrs[j];
+  void *d_table = nullptr;
+  RSB_CU(cudaMallocAsync(&d_table, table.size() * sizeof(void *), st));
+  RSB_CU(cudaMemcpyAsync(d_table, table.data(), table.size() * sizeof(void *), cudaMemcpyHostToDevice, st));
+  Apply16Args a{};
+  a.in_ptrs = reinterpret_cast<const uint8_t *const *>(d_table);
+  a.out_ptrs = reinterpret_cast<uint8_t *const *>(static_cast<char *>(d_table) + k * sizeof(void *));
+  a.coeffs = coeffs;
+  a.k = k;
+  a.rows = rows;
+  a.n_sym = len / 2;
+  a.n_stripes = 1;
+  a.mismatch = mismatch;
+  int st_ = launch_gf16(a, verify, st);
+  cudaFreeAsync(d_table, st);
+  return st_;
+}
+
+static int reconstruct16(const Gen16 &g, PlanCache *cache, const Plan *fixed, Exec &ex,
+                         uint8_t *const *shards, const size_t *lens, const uint8_t *present,
+                         size_t n_shards, bool data_only, bool dev, cudaStream_t st) {
+  size_t n = g.k + g.m;
+  if (!shards || !lens || !present) return RS_ERR_INVALID_ARGUMENT;
+  if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
+  Presence pres;
+  size_t n_present = 0, len = 0;
+  RSB_TRY(scan_shards(lens, present, n, true, pres, n_present, len));
+  if (fixed && pres != fixed->presence) return RS_INVALID_SHARD_FLAGS;
+  if (n_present == n) return RS_OK;
+  if (!fixed && n_present < g.k) return RS_TOO_FEW_SHARDS_PRESENT;
+  if (len == 0) return RS_TOO_FEW_SHARDS_PRESENT;
+  std::shared_ptr<const Plan> hold;
+  const Plan *plan = fixed;
+  if (!plan) {
+    RSB_TRY(plan16_for(g, *cache, pres, hold));
+    plan = hold.get();
+  }
+  RSB_TRY(check_absent_buffers(lens, present, n, g.k, len, data_only));
+  size_t rows = plan->missing_data.size() + (data_only ? 0 : plan->missing_parity.size());
+  if (rows == 0) return RS_OK;
+  std::vector<uint32_t> outs(plan->missing_data);
+  if (!data_only) outs.insert(outs.end(), plan->missing_parity.begin(), plan->missing_parity.end());
+  const uint32_t *coeffs = reinterpret_cast<const uint32_t *>(plan->d_rows);
+  if (dev) {
+    RSB_CU(cudaSetDevice(g.device));
+    std::vector<const uint8_t *> ins(g.k);
+    std::vector<uint8_t *> os(rows);
+    for (size_t t = 0; t < g.k; t++) ins[t] = shards[plan->survivors[t]];
+    for (size_t j = 0; j < rows; j++) os[j] = shards[outs[j]];
+    return apply16_ptrs(coeffs, (uint32_t)g.k, (uint32_t)rows, ins.data(), os.data(), len, false, nullptr, st);
+  }
+  std::lock_guard<std::mutex> lock(ex.mu);
+  RSB_CU(cudaSetDevice(g.device));
+  RSB_TRY(ex.buf.ensure((g.k + rows) * len));
+  for (size_t t = 0; t < g.k; t++)
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + t * len, shards[plan->survivors[t]], len, cudaMemcpyHostToDevice,
+                           ex.stream));
+  Apply16Args a{};
+  a.in_base = ex.buf.ptr;
+  a.in_row_stride = len;
+  a.out_base = ex.buf.ptr + g.k * len;
+  a.out_row_stride = len;
+  a.coeffs = coeffs;
+  a.k = (uint32_t)g.k;
+  a.rows = (uint32_t)rows;
+  a.n_sym = len / 2;
+  a.n_stripes = 1;
+  RSB_TRY(launch_gf16(a, false, ex.stream));
+  for (size_t j = 0; j < rows; j++)
+    RSB_CU(cudaMemcpyAsync(shards[outs[j]], ex.buf.ptr + (g.k + j) * len, len, cudaMemcpyDeviceToHost,
+                           ex.stream));
+  RSB_CU(cudaStreamSynchronize(ex.stream));
+  return RS_OK;
+}
+
+}  // namespace rsb
+
+extern "C" {
+
+int rs16_new(size_t k, size_t m, rs16_t **out) {
+  if (!out) return RS_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (k == 0) return RS_TOO_FEW_DATA_SHARDS;
+  if (m == 0) return RS_TOO_FEW_PARITY_SHARDS;
+  if (k + m > 65536) return RS_TOO_MANY_SHARDS;
+  int dev = 0;
+  RSB_TRY(ensure_device(&dev));
+  auto gen = std::make_shared<Gen16>();
+  gen->device = dev;
+  gen->k = k;
+  gen->m = m;
+  parity_rows<F16>(k, m, gen->rows);
+  uint32_t *d = nullptr;
+  RSB_TRY(upload_split(gen->rows, &d));
+  gen->d_split = d;
+  auto c = new (std::nothrow) rs16_codec();
+  if (!c) return RS_ERR_ALLOC;
+  c->gen = gen;
+  c->plans = std::make_shared<PlanCache>();
+  int st = make_exec(dev, c->exec);
+  if (st) {
+    delete c;
+    return st;
+  }
+  *out = c;
+  return RS_OK;
+}
+
+int rs16_clone(const rs16_t *codec, rs16_t **out) {
+  if (!codec || !out) return RS_ERR_INVALID_ARGUMENT;
+  auto c = new (std::nothrow) rs16_codec();
+  if (!c) return RS_ERR_ALLOC;
+  c->gen = codec->gen;
+  c->plans = std::make_shared<PlanCache>();
+  c->plans->copy_from(*codec->plans);
+  int st = make_exec(codec->gen->device, c->exec);
+  if (st) {
+    delete c;
+    return st;
+  }
+  *out = c;
+  return RS_OK;
+}
+
+void rs16_free(rs16_t *codec) { delete codec; }
+size_t rs16_data_shard_count(const rs16_t *c) { return c ? c->gen->k : 0; }
+size_t rs16_parity_shard_count(const rs16_t *c) { return c ? c->gen->m : 0; }
+size_t rs16_total_shard_count(const rs16_t *c) { return c ? c->gen->k + c->gen->m : 0; }
+int rs16_equal(const rs16_t *a, const rs16_t *b) {
+  if (!a || !b) return 0;
+  return a->gen->k == b->gen->k && a->gen->m == b->gen->m;
+}
+
+int rs16_parity_matrix(const rs16_t *c, uint16_t *out, size_t out_len) {
+  if (!c || !out) return RS_ERR_INVALID_ARGUMENT;
+  if (out_len != c->gen->rows.size()) return RS_INCORRECT_SHARD_SIZE;
+  memcpy(out, c->gen->rows.data(), out_len * 2);
+  return RS_OK;
+}
+
+const char *rs16_encode_route(const rs16_t *c) {
+  (void)c;
+  return "matrix";
+}
+
+// src/reedsolomon16.rs:412-419
+int rs16_encode(rs16_t *c, uint8_t *const *shards, size_t n_shards, size_t len) {
+  if (!c || !shards) return RS_ERR_INVALID_ARGUMENT;
+  const Gen16 &g = *c->gen;
+  size_t n = g.k + g.m;
+  if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
+  RSB_TRY(check_len16(len));
+  Exec &ex = *c->exec;
+  std::lock_guard<std::mutex> lock(ex.mu);
+  RSB_CU(cudaSetDevice(g.device));
+  RSB_TRY(ex.buf.ensure(n * len));
+  for (size_t i = 0; i < g.k; i++)
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * len, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
+  Apply16Args a{};
+  a.in_base = ex.buf.ptr;
+  a.in_row_stride = len;
+  a.out_base = ex.buf.ptr + g.k * len;
+  a.out_row_stride = len;
+  a.coeffs = g.d_split;
+  a.k = (uint32_t)g.k;
+  a.rows = (uint32_t)g.m;
+  a.n_sym = len / 2;
+  a.n_stripes = 1;
+  RSB_TRY(launch_gf16(a, false, ex.stream));
+  for (size_t j = 0; j < g.m; j++)
+    RSB_CU(cudaMemcpyAsync(shards[g.k + j], ex.buf.ptr + (g.k + j) * len, len, cudaMemcpyDeviceToHost,
+                           ex.stream));
+  RSB_CU(cudaStreamSynchronize(ex.stream));
+  return RS_OK;
+}
+
+// src/reedsolomon16.rs:422-446
+int rs16_encode_sep(rs16_t *c, const uint8_t *const *data, size_t n_data, uint8_t *const *parity,
+                    size_t n_parity, size_t len) {
+  if (!c || !data || !parity) return RS_ERR_INVALID_ARGUMENT;
+  const Gen16 &g = *c->gen;
+  if (n_data != g.k) return n_data < g.k ? RS_TOO_FEW_DATA_SHARDS : RS_TOO_MANY_DATA_SHARDS;
+  if (n_parity != g.m) return n_parity < g.m ? RS_TOO_FEW_PARITY_SHARDS : RS_TOO_MANY_PARITY_SHARDS;
+  RSB_TRY(check_len16(len));
+  std::vector<uint8_t *> all(g.k + g.m);
+  for (size_t i = 0; i < g.k; i++) all[i] = const_cast<uint8_t *>(data[i]);
+  for (size_t j = 0; j < g.m; j++) all[g.k + j] = parity[j];
+  return rs16_encode(c, all.data(), all.size(), len);
+}
+
+// src/reedsolomon16.rs:450-505
+int rs16_verify(rs16_t *c, const uint8_t *const *shards, size_t n_shards, size_t len, int *ok) {
+  if (!c || !shards || !ok) return RS_ERR_INVALID_ARGUMENT;
+  const Gen16 &g = *c->gen;
+  size_t n = g.k + g.m;
+  if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
+  RSB_TRY(check_len16(len));
+  Exec &ex = *c->exec;
+  std::lock_guard<std::mutex> lock(ex.mu);
+  RSB_CU(cudaSetDevice(g.device));
+  RSB_TRY(ex.buf.ensure(n * len));
+  RSB_TRY(ex.aux.ensure(64));
+  for (size_t i = 0; i < n; i++)
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * len, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
+  uint32_t *flag = reinterpret_cast<uint32_t *>(ex.aux.ptr);
+  RSB_CU(cudaMemsetAsync(flag, 0, 4, ex.stream));
+  Apply16Args a{};
+  a.in_base = ex.buf.ptr;
+  a.in_row_stride = len;
+  a.out_base = ex.buf.ptr + g.k * len;
+  a.out_row_stride = len;
+  a.coeffs = g.d_split;
+  a.k = (uint32_t)g.k;
+  a.rows = (uint32_t)g.m;
+  a.n_sym = len / 2;
+  a.n_stripes = 1;
+  a.mismatch = flag;
+  RSB_TRY(launch_gf16(a, true, ex.stream));
+  uint32_t h = 0;
+  RSB_CU(cudaMemcpyAsync(&h, flag, 4, cudaMemcpyDeviceToHost, ex.stream));
+  RSB_CU(cudaStreamSynchronize(ex.stream));
+  *ok = h ? 0 : 1;
+  return RS_OK;
+}
+
+int rs16_reconstruct(rs16_t *c, uint8_t *const *shards, const size_t *lens, const uint8_t *present,
+                     size_t n_shards, int data_only) {
+  if (!c) return RS_ERR_INVALID_ARGUMENT;
+  return reconstruct16(*c->gen, c->plans.get(), nullptr, *c->exec, shards, lens, present, n_shards,
+                       data_only != 0, false, nullptr);
+}
+
+// src/reedsolomon16.rs:544-565
+int rs16_reconstruct_rows(rs16_t *c, uint8_t *rows, size_t rows_len, size_t row_len,
+                          const uint8_t *present, size_t n_present) {
+  if (!c || !present) return RS_ERR_INVALID_ARGUMENT;
+  size_t n = c->gen->k + c->gen->m;
+  if (n_present != n) return RS_INVALID_SHARD_FLAGS;
+  if (row_len == 0 || row_len % 2) return RS_INCORRECT_SHARD_SIZE;
+  if (rows_len != n * row_len) return RS_INCORRECT_SHARD_SIZE;
+  if (!rows) return RS_ERR_INVALID_ARGUMENT;
+  std::vector<uint8_t *> shards(n);
+  std::vector<size_t> lens(n, row_len);
+  for (size_t i = 0; i < n; i++) shards[i] = rows + i * row_len;
+  return rs16_reconstruct(c, shards.data(), lens.data(), present, n, 0);
+}
+
+// src/reedsolomon16.rs:518-541
+int rs16_prepare_decode(rs16_t *c, const uint8_t *present, size_t n_present, rs16_dec_t **out) {
+  if (!c || !out) return RS_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  const Gen16 &g = *c->gen;
+  size_t n = g.k + g.m;
+  if (n_present != n) return RS_INVALID_SHARD_FLAGS;
+  if (!present) return RS_ERR_INVALID_ARGUMENT;
+  Presence pres(n);
+  size_t count = 0;
+  for (size_t i = 0; i < n; i++)
+    if (present[i]) {
+      pres.set(i);
+      count++;
+    }
+  if (count < g.k) return RS_TOO_FEW_SHARDS_PRESENT;
+  std::shared_ptr<const Plan> plan;
+  RSB_TRY(plan16_for(g, *c->plans, pres, plan));
+  auto d = new (std::nothrow) rs16_decoder();
+  if (!d) return RS_ERR_ALLOC;
+  d->gen = c->gen;
+  d->plan = plan;
+  d->exec = c->exec;
+  *out = d;
+  return RS_OK;
+}
+
+int rs16_dec_reconstruct(rs16_dec_t *d, uint8_t *const *shards, const size_t *lens, const uint8_t *present,
+                         size_t n_shards, int data_only) {
+  if (!d) return RS_ERR_INVALID_ARGUMENT;
+  return reconstruct16(*d->gen, nullptr, d->plan.get(), *d->exec, shards, lens, present, n_shards,
+                       data_only != 0, false, nullptr);
+}
+
+int rs16_dec_clone(const rs16_dec_t *d, rs16_dec_t **out) {
+  if (!d || !out) return RS_ERR_INVALID_ARGUMENT;
+  auto c = new (std::nothrow) rs16_decoder(*d);
+  if (!c) return RS_ERR_ALLOC;
+  *out = c;
+  return RS_OK;
+}
+
+void rs16_dec_free(rs16_dec_t *d) { delete d; }
+
+int rs16_encode_dev(rs16_t *c, uint8_t *const *d_shards, size_t n_shards, size_t len, void *stream) {
+  if (!c || !d_shards) return RS_ERR_INVALID_ARGUMENT;
+  const Gen16 &g = *c->gen;
+  size_t n = g.k + g.m;
+  if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
+  RSB_TRY(check_len16(len));
+  RSB_CU(cudaSetDevice(g.device));
+  return apply16_ptrs(g.d_split, (uint32_t)g.k, (uint32_t)g.m, d_shards, d_shards + g.k, len, false, nullptr,
+                      (cudaStream_t)stream);
+}
+
+int rs16_encode_batch_dev(rs16_t *c, const uint8_t *d_data, size_t data_stride, uint8_t *d_parity,
+                          size_t parity_stride, size_t n_stripes, size_t row_len, void *stream) {
+  if (!c) return RS_ERR_INVALID_ARGUMENT;
+  if (n_stripes == 0) return RS_OK;
+  RSB_TRY(check_len16(row_len));
+  if (!d_data || !d_parity) return RS_ERR_INVALID_ARGUMENT;
+  const Gen16 &g = *c->gen;
+  RSB_CU(cudaSetDevice(g.device));
+  Apply16Args a{};
+  a.in_base = d_data;
+  a.in_row_stride = row_len;
+  a.in_stripe_stride = data_stride;
+  a.out_base = d_parity;
+  a.out_row_stride = row_len;
+  a.out_stripe_stride = parity_stride;
+  a.coeffs = g.d_split;
+  a.k = (uint32_t)g.k;
+  a.rows = (uint32_t)g.m;
+  a.n_sym = row_len / 2;
+  a.n_stripes = (uint32_t)n_stripes;
+  return launch_gf16(a, false, (cudaStream_t)stream);
+}
+
+int rs16_reconstruct_dev(rs16_t *c, uint8_t *const *d_shards, const size_t *lens, const uint8_t *present,
+                         size_t n_shards, int data_only, void *stream) {
+  if (!c) return RS_ERR_INVALID_ARGUMENT;
+  return reconstruct16(*c->gen, c->plans.get(), nullptr, *c->exec, d_shards, lens, present, n_shards,
+                       data_only != 0, true, (cudaStream_t)stream);
+}
+
+}  // extern "C"

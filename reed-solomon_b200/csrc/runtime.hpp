@@ -1,0 +1,198 @@
+// Shared runtime pieces of the rs_b200 library: status handling, device buffers,
+// per-codec execution contexts, presence masks and the decode-plan cache.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <shared_mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "rs_b200.h"
+
+namespace rsb {
+
+extern std::atomic<uint64_t> g_launches;
+void set_cuda_error(cudaError_t e, const char *what);
+int ensure_device(int *device_out);
+
+#define RSB_CU(call)                          \
+  do {                                        \
+    cudaError_t e_ = (call);                  \
+    if (e_ != cudaSuccess) {                  \
+      ::rsb::set_cuda_error(e_, #call);       \
+      return RS_ERR_CUDA;                     \
+    }                                         \
+  } while (0)
+
+#define RSB_TRY(expr)           \
+  do {                          \
+    int st_ = (expr);           \
+    if (st_ != RS_OK) return st_; \
+  } while (0)
+
+// Grow-only device allocation owned by one execution context.
+struct DeviceBuf {
+  uint8_t *ptr = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return RS_OK;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    size_t want = std::max(bytes, (size_t)1 << 20);
+    if (cudaMalloc(&ptr, want) != cudaSuccess) {
+      cudaGetLastError();
+      return RS_ERR_ALLOC;
+    }
+    cap = want;
+    return RS_OK;
+  }
+  ~DeviceBuf() {
+    if (ptr) cudaFree(ptr);
+  }
+};
+
+// Serialises host-pointer calls on one codec and owns their staging memory.
+struct Exec {
+  static constexpr int kPipe = 3;  // streams of the pipelined host batch path
+  int device = 0;
+  std::mutex mu;
+  DeviceBuf buf;
+  DeviceBuf aux;
+  DeviceBuf pipe_buf;
+  cudaStream_t stream = nullptr;
+  cudaStream_t pipe[kPipe] = {nullptr, nullptr, nullptr};
+  ~Exec() {
+    if (stream) cudaStreamDestroy(stream);
+    for (auto s : pipe)
+      if (s) cudaStreamDestroy(s);
+  }
+  int pipe_streams() {
+    for (auto &s : pipe)
+      if (!s) RSB_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return RS_OK;
+  }
+  int init(int dev) {
+    device = dev;
+    RSB_CU(cudaSetDevice(dev));
+    RSB_CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    return RS_OK;
+  }
+};
+
+inline int make_exec(int device, std::shared_ptr<Exec> &out) {
+  auto e = std::make_shared<Exec>();
+  RSB_TRY(e->init(device));
+  out = e;
+  return RS_OK;
+}
+
+// Which shard slots are present, one bit per index (src/reedsolomon.rs:103-115).
+struct Presence {
+  std::vector<uint64_t> bits;
+  explicit Presence(size_t n = 0) : bits((n + 63) / 64, 0) {}
+  void set(size_t i) { bits[i / 64] |= 1ull << (i % 64); }
+  bool get(size_t i) const { return (bits[i / 64] >> (i % 64)) & 1; }
+  bool operator==(const Presence &o) const { return bits == o.bits; }
+  bool operator!=(const Presence &o) const { return bits != o.bits; }
+};
+
+// One erasure pattern's plan: survivors (first k present, ascending), the missing
+// indexes (data ascending, then parity ascending) and device rows mapping the
+// survivors to each missing shard, in that order.
+struct Plan {
+  Presence presence;
+  std::vector<uint32_t> survivors, missing_data, missing_parity;
+  int device = 0;
+  void *d_rows = nullptr;  // rows x k coefficients (u8 for GF(2^8), split u32 for the tower)
+  ~Plan() {
+    if (d_rows) {
+      cudaSetDevice(device);
+      cudaFree(d_rows);
+    }
+  }
+};
+
+// Recently used plans, most recent first, at most 64 (src/reedsolomon.rs:24,592-613).
+struct PlanCache {
+  static constexpr size_t kLimit = 64;
+  std::shared_mutex mu;
+  std::vector<std::pair<Presence, std::shared_ptr<const Plan>>> list;
+  std::shared_ptr<const Plan> find(const Presence &p) {
+    std::shared_lock<std::shared_mutex> lock(mu);
+    for (auto &e : list)
+      if (e.first == p) return e.second;
+    return nullptr;
+  }
+  std::shared_ptr<const Plan> insert(const Presence &p, std::shared_ptr<const Plan> plan) {
+    std::unique_lock<std::shared_mutex> lock(mu);
+    for (auto &e : list)
+      if (e.first == p) return e.second;  // a racing thread won; reuse its plan
+    list.insert(list.begin(), {p, plan});
+    if (list.size() > kLimit) list.resize(kLimit);
+    return plan;
+  }
+  void copy_from(PlanCache &o) {
+    std::shared_lock<std::shared_mutex> lock(o.mu);
+    list = o.list;
+  }
+};
+
+// Presence scan of reconstruct, src/reedsolomon.rs:801-821 (GF(2^8)) and
+// src/reedsolomon16.rs:690-703 (tower: even lengths only).
+inline int scan_shards(const size_t *lens, const uint8_t *present, size_t n, bool even,
+                       Presence &pres, size_t &n_present, size_t &shard_len) {
+  pres = Presence(n);
+  n_present = 0;
+  shard_len = 0;
+  for (size_t i = 0; i < n; i++) {
+    if (!present[i]) continue;
+    size_t len = lens[i];
+    if (len == 0) return RS_EMPTY_SHARD;
+    if (even && (len % 2)) return RS_INCORRECT_SHARD_SIZE;
+    if (shard_len && shard_len != len) return RS_INCORRECT_SHARD_SIZE;
+    shard_len = len;
+    pres.set(i);
+    n_present++;
+  }
+  return RS_OK;
+}
+
+// Survivors and missing lists of a pattern, src/reedsolomon.rs:550-566.
+inline void split_pattern(const Presence &p, size_t k, size_t n, std::vector<uint32_t> &surv,
+                          std::vector<uint32_t> &md, std::vector<uint32_t> &mp) {
+  surv.clear();
+  md.clear();
+  mp.clear();
+  for (size_t i = 0; i < n; i++) {
+    if (p.get(i)) {
+      if (surv.size() < k) surv.push_back((uint32_t)i);
+    } else if (i < k) {
+      md.push_back((uint32_t)i);
+    } else {
+      mp.push_back((uint32_t)i);
+    }
+  }
+}
+
+// Buffer gather of reconstruct_with_plan, src/reedsolomon.rs:837-864: an absent
+// buffer that will be written must already have the shard length (absent parity
+// buffers are skipped when only data is rebuilt).
+inline int check_absent_buffers(const size_t *lens, const uint8_t *present, size_t n, size_t k,
+                                size_t shard_len, bool data_only) {
+  for (size_t i = 0; i < n; i++) {
+    if (present[i]) continue;
+    if (i >= k && data_only) continue;
+    if (lens[i] != shard_len) return RS_INCORRECT_SHARD_SIZE;
+  }
+  return RS_OK;
+}
+
+}  // namespace rsb

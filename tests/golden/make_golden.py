@@ -168,8 +168,13 @@ def main():
         [int(c, 0), [int(v) if v.strip().isdigit() else {"TOWER_L": 32}[v.strip()] for v in row.split(",")]]
         for c, row in cm
     ]
+    errors = read(root, "src/errors.rs")
+    variants = re.findall(r"^\s+(\w+),$", errors[errors.index("pub enum Error"): errors.index("}")], re.M)
+    messages = dict(re.findall(r'Error::(\w+) => "([^"]*)"', errors))
     vectors = {
         "source": "spool-labs/reed-solomon (tape-reed-solomon 0.2.2), read as text",
+        "error_variants": variants,
+        "error_messages": [messages[v] for v in variants],
         "backblaze_log_table": backblaze_table(galois),
         "known_mul": muls,
         "known_exp": exps,

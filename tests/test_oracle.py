@@ -1,0 +1,153 @@
+"""The CPU oracle against the reference's own golden vectors and known answers.
+
+These pin the oracle before any GPU result is compared with it:
+* src/galois.rs:119-163   Backblaze log table, known products, field axioms
+* src/galois16.rs:143-233 tower constant, const_matrix, inverses
+* src/reedsolomon16.rs:1087-1101 frozen wire vector
+* src/fft_programs.rs     the reference's generated programs: digests, counts, outputs
+* src/fft.rs:890-1103     FFT/IFFT shape tests, programs == matrix encode, op counts
+* src/matrix.rs:205-236   Vandermonde inverse, singular matrix
+"""
+import numpy as np
+import pytest
+
+
+def test_log_table_same_as_backblaze(O, golden):
+    log, _ = O.gf8_tables()
+    assert list(log) == golden["backblaze_log_table"]
+
+
+def test_known_products(O, golden):
+    assert golden["known_mul"] and golden["known_exp"]
+    for a, b, c in golden["known_mul"]:
+        assert O.gf8_mul(a, b) == c
+    for a, n, c in golden["known_exp"]:
+        assert O.gf8_exp(a, n) == c
+
+
+def test_field_axioms(O):
+    t = O.gf8_mul_table()
+    assert np.array_equal(t, t.T)
+    for a in range(1, 256):
+        assert O.gf8_mul(a, O.gf8_div(1, a)) == 1
+    with pytest.raises(ZeroDivisionError):
+        O.gf8_div(3, 0)
+
+
+def _trace(O, x):
+    acc = 0
+    for _ in range(8):
+        acc ^= x
+        x = O.gf8_mul(x, x)
+    return acc
+
+
+def test_tower_constant_smallest_trace_one(O, golden):
+    L = golden["gf16_tower_l"]
+    assert all(_trace(O, c) == 0 for c in range(L))
+    assert _trace(O, L) == 1
+    assert sum(_trace(O, c) for c in range(256)) == 128
+
+
+def test_const_matrix(O, golden):
+    for c, want in golden["gf16_const_matrix"]:
+        assert O.gf16_const_matrix(c) == want
+    rng = np.random.default_rng(5)
+    for c in list(range(0, 65536, 97)) + [0xFFFF, 0x0100, 32]:
+        m = O.gf16_const_matrix(c)
+        for a in rng.integers(0, 65536, size=6).tolist() + [0, 1, 0xFFFF]:
+            ah, al = a >> 8, a & 0xFF
+            hi = O.gf8_mul(m[0], ah) ^ O.gf8_mul(m[1], al)
+            lo = O.gf8_mul(m[2], ah) ^ O.gf8_mul(m[3], al)
+            assert (hi << 8 | lo) == O.gf16_mul(c, a)
+
+
+def test_gf16_all_inverses(O):
+    for a in range(1, 65536):
+        assert O.gf16_mul(a, O.gf16_inv(a)) == 1
+
+
+def test_gf16_wire_vector(O, golden):
+    g = golden["gf16_wire_vector"]
+    data = np.array(g["data"], np.uint8)
+    assert O.encode16(g["k"], g["m"], data).tolist() == g["parity"]
+
+
+@pytest.mark.parametrize("idx", range(6))
+def test_fft_programs_match_reference(O, golden, idx):
+    p = golden["fft_programs"][idx]
+    k, m = p["k"], p["m"]
+    ops, regs, _, mults = O.fft_flat_program(k, m)
+    assert regs == p["registers"]
+    assert len(ops) == p["ops_body"] == p["ops_header"]
+    assert mults == p["multiplies"]
+    assert O.fft_program_digest(k, m) == p["sha256"]
+    cols = np.array(p["columns"], np.uint8)
+    for col, want in zip(cols, p["parity"]):
+        assert O.fft_flat_run(k, m, col).tolist() == want
+        assert O.fft_staged_run(k, m, col).tolist() == want
+    # The matrix encode equals the reference programs' outputs.
+    assert O.encode8(k, m, cols.T.copy()).T.tolist() == p["parity"]
+
+
+def test_what_tables(O):
+    what = O.fft_what().astype(np.int64)
+    for level in range(8):
+        assert (what[level, : 1 << level] == 0).all()
+        assert what[level, 1 << level] == 1
+        for a in range(256):
+            assert what[level, a ^ 0x5A] == what[level, a] ^ what[level, 0x5A]
+
+
+# src/fft.rs:963-985 shape list
+SHAPES = [(1, 1), (1, 4), (2, 2), (3, 5), (4, 2), (5, 3), (6, 4), (7, 13), (9, 3), (10, 10),
+          (10, 7), (11, 5), (13, 7), (14, 14), (16, 4), (17, 17), (18, 6), (20, 10), (24, 8),
+          (32, 32), (37, 21)]
+
+
+@pytest.mark.parametrize("k,m", SHAPES)
+def test_programs_match_matrix(O, k, m):
+    rng = np.random.default_rng(k * 131 + m)
+    data = rng.integers(0, 256, size=(k, 64), dtype=np.uint8)
+    want = O.encode8(k, m, data)
+    for b in range(64):
+        assert O.fft_flat_run(k, m, data[:, b]).tolist() == want[:, b].tolist()
+        assert O.fft_staged_run(k, m, data[:, b]).tolist() == want[:, b].tolist()
+
+
+def test_program_op_counts(O):
+    for k, m in [(7, 13), (10, 10), (14, 14), (16, 16), (18, 6)]:
+        _, _, _, mults = O.fft_flat_program(k, m)
+        assert mults < k * m
+        assert O.fft_staged_stats(k, m)["mult_count"] < k * m
+
+
+@pytest.mark.parametrize("field,size", [(8, 20), (16, 86)])
+def test_vandermonde_inverse_is_identity(O, field, size):
+    v = O.vandermonde(field, size, size)
+    st, inv = O.invert(field, v)
+    assert st == 0
+    assert np.array_equal(O.matmul(field, v, inv), np.eye(size, dtype=np.uint16))
+
+
+def test_singular_matrix_errors(O):
+    st, _ = O.invert(16, np.ones((2, 2), np.uint16))
+    assert st == 14
+
+
+@pytest.mark.parametrize("field", [8, 16])
+def test_oracle_reconstruct_round_trip(O, field):
+    rng = np.random.default_rng(field)
+    for k, m in [(4, 2), (7, 13), (10, 10)]:
+        length = 64
+        data = rng.integers(0, 256, size=(k, length), dtype=np.uint8)
+        par = O.encode8(k, m, data) if field == 8 else O.encode16(k, m, data)
+        full = np.concatenate([data, par])
+        for e in range(1, m + 1):
+            erased = rng.choice(k + m, size=e, replace=False)
+            rows = full.copy()
+            rows[erased] = 0
+            present = np.ones(k + m, np.uint8)
+            present[erased] = 0
+            assert O.reconstruct(field, k, m, rows, present) == 0
+            assert np.array_equal(rows, full)
