@@ -32,15 +32,29 @@ __device__ __forceinline__ uint8_t gmul_tab(const uint8_t *lg, const uint8_t *ex
   return (a && b) ? ex[lg[a] + lg[b]] : 0;
 }
 
-// Dynamic shared memory: 768 B tables + k*2k matrix + k factors + pivot slot.
+// Dynamic shared memory layout: 768 B of log/exp tables, the k x 2k matrix, k pivot
+// factors and the pivot slot, each region starting on a 16-byte boundary.
+struct PlanSmem {
+  uint32_t f_off, piv_off, total;
+};
+__host__ __device__ inline PlanSmem plan_smem(uint32_t k) {
+  auto up = [](uint32_t x) { return (x + 15u) & ~15u; };
+  PlanSmem s;
+  s.f_off = up(768 + 2 * k * k);
+  s.piv_off = up(s.f_off + k);
+  s.total = s.piv_off + 16;
+  return s;
+}
+
 static __global__ void __launch_bounds__(256) gf8_plan_kernel(const PlanArgs a) {
   extern __shared__ __align__(16) uint8_t sm[];
   uint8_t *lg = sm;          // 256
   uint8_t *ex = sm + 256;    // 512
   const uint32_t k = a.k, w = 2 * k;
+  const PlanSmem lay = plan_smem(k);
   uint8_t *A = sm + 768;     // k x 2k
-  uint8_t *f = A + k * w;    // k factors
-  int *piv = reinterpret_cast<int *>(f + ((k + 15) & ~15u));
+  uint8_t *f = sm + lay.f_off;  // k factors
+  int *piv = reinterpret_cast<int *>(sm + lay.piv_off);
   const uint32_t p = blockIdx.x;
   if (threadIdx.x == 0) {
     unsigned x = 1;

@@ -205,7 +205,7 @@ static int plan8_for(const Gen8 &g, PlanCache &cache, Exec &ex, const Presence &
   pa.max_rows = (uint32_t)std::max<size_t>(rows, 1);
   pa.out = reinterpret_cast<uint8_t *>(d_rows);
   pa.status = d_status;
-  size_t smem = 768 + g.k * 2 * g.k + ((g.k + 15) & ~size_t(15)) + 16;
+  size_t smem = plan_smem((uint32_t)g.k).total;
   if (smem > 48 * 1024)
     RSB_CU(cudaFuncSetAttribute(gf8_plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   gf8_plan_kernel<<<1, 256, smem, ex.stream>>>(pa);
@@ -806,7 +806,7 @@ int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, s
   pa.max_rows = (uint32_t)g.m;
   pa.out = base + o_rows;
   pa.status = reinterpret_cast<int *>(base + o_stat);
-  size_t smem = 768 + k * 2 * k + ((k + 15) & ~size_t(15)) + 16;
+  size_t smem = plan_smem((uint32_t)k).total;
   if (smem > 48 * 1024)
     RSB_CU(cudaFuncSetAttribute(gf8_plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   gf8_plan_kernel<<<(unsigned)n_stripes, 256, smem, st>>>(pa);
