@@ -142,9 +142,11 @@ __device__ __forceinline__ void level_local(Reg (&r)[K / 2]) {
   });
 }
 
-// Level 0 across the lane pair. hmask is 0 on lane 0 (even registers), ~0 on lane 1.
+// Level 0 across the lane pair; h1 is 0 on lane 0 (even registers) and 1 on lane 1,
+// h0 = 1 - h1. Lane selects are written as integer multiply-adds by 0/1 so they issue
+// on the FMA pipe, which the LOP3-heavy butterflies leave idle.
 template <int K, int BETA, bool INV>
-__device__ __forceinline__ void level0_pair(Reg (&r)[K / 2], uint32_t hmask) {
+__device__ __forceinline__ void level0_pair(Reg (&r)[K / 2], uint32_t h0, uint32_t h1) {
   static_for<0, K / 2>([&](auto jj) {
     constexpr int j = decltype(jj)::value;
     constexpr uint8_t c = kWhat.v[0][BETA ^ (2 * j)];
@@ -164,12 +166,12 @@ __device__ __forceinline__ void level0_pair(Reg (&r)[K / 2], uint32_t hmask) {
       else if constexpr (c != 0)
         mul_acc<c>(v, t);
 #pragma unroll
-      for (int b = 0; b < 8; b++) r[j][b] = (t[b] & hmask) | (v[b] & ~hmask);
+      for (int b = 0; b < 8; b++) r[j][b] = t[b] * h1 + v[b] * h0;
     } else {
       // lo' = lo ^ c*hi; hi' = hi ^ lo'. Lane 0: own ^ c*p; lane 1: own ^ p ^ c*own.
       Reg z, u;
 #pragma unroll
-      for (int b = 0; b < 8; b++) z[b] = (r[j][b] & hmask) | (p[b] & ~hmask);
+      for (int b = 0; b < 8; b++) z[b] = r[j][b] * h1 + p[b] * h0;
       if constexpr (c == 1) {
 #pragma unroll
         for (int b = 0; b < 8; b++) u[b] = z[b];
@@ -180,7 +182,7 @@ __device__ __forceinline__ void level0_pair(Reg (&r)[K / 2], uint32_t hmask) {
         for (int b = 0; b < 8; b++) u[b] = 0;
       }
 #pragma unroll
-      for (int b = 0; b < 8; b++) r[j][b] ^= u[b] ^ (p[b] & hmask);
+      for (int b = 0; b < 8; b++) r[j][b] ^= u[b] ^ (p[b] * h1);
     }
   });
 }
@@ -275,56 +277,120 @@ struct FftArgs {
 };
 
 constexpr int kFftThreads = 128;
+constexpr int kFftCtasPerSm = 3;
 
-// grid.x covers (stripes x groups) lane pairs; one lane pair per 32-column group.
+// Per-thread staging of one 32-column group in shared memory: shard slot j, half q
+// (16 bytes each) of thread t sits at j*kFftSlot + q*kFftHalf + t*16, so a warp's
+// 16-byte accesses to one (j, q) are contiguous and free of bank conflicts.
+constexpr int kFftHalf = kFftThreads * 16;
+constexpr int kFftSlot = 2 * kFftHalf;
+
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
+  uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Stage the 32 bytes at p (remain of them valid) into this thread's slot: two async
+// 16-byte copies when aligned and whole, else a zero-filled byte path.
+__device__ __forceinline__ void stage32(uint8_t *slot, const uint8_t *p, uint64_t remain) {
+  if (remain >= 32 && (((uintptr_t)p & 15u) == 0)) {
+    cp_async16(slot, p);
+    cp_async16(slot + kFftHalf, p + 16);
+  } else {
+    uint32_t w[8];
+    load32(p, remain, w);
+    *reinterpret_cast<uint4 *>(slot) = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4 *>(slot + kFftHalf) = make_uint4(w[4], w[5], w[6], w[7]);
+  }
+}
+
+// Persistent lane pairs: round r handles group pair0 + r*stride of the flattened
+// (stripe, 32-column group) space. The next round's 32 bytes per shard are copied
+// into shared memory with cp.async while the current round computes. Every lane runs
+// every round (on zeros past the end) so each shuffle sees the full warp.
 template <int K, bool PTRS>
-__global__ void __launch_bounds__(kFftThreads)
+__global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm)
     fft_kk_kernel(const FftArgs a, const __grid_constant__ PtrTableT<PTRS> pt) {
+  extern __shared__ __align__(16) uint8_t stage[];
   using namespace fftc;
-  const uint64_t pair = ((uint64_t)blockIdx.x * kFftThreads + threadIdx.x) >> 1;
-  const uint32_t h = threadIdx.x & 1;
-  const uint32_t hmask = h ? 0xffffffffu : 0u;
+  const uint32_t tid = threadIdx.x;
+  const uint32_t h1 = tid & 1, h0 = 1 - h1;
   const uint64_t total = (uint64_t)a.n_stripes * a.groups_per_stripe;
-  // Pairs past the end still run (on zeros) so every shuffle sees the full warp.
-  const bool live = pair < total;
-  const uint32_t s = live ? (uint32_t)(pair / a.groups_per_stripe) : 0;
-  const uint64_t col = live ? (pair % a.groups_per_stripe) * 32 : 0;
-  const uint64_t remain = live ? a.len - col : 0;
-  Reg r[K / 2];
-#pragma unroll
-  for (int j = 0; j < K / 2; j++) {
-    const uint8_t *row;
+  const uint64_t stride = (uint64_t)gridDim.x * (kFftThreads / 2);
+  const uint64_t rounds = (total + stride - 1) / stride;
+  const uint64_t pair0 = ((uint64_t)blockIdx.x * kFftThreads + tid) >> 1;
+  uint8_t *mine = stage + tid * 16;
+
+  auto in_ptr = [&](uint32_t s, int j) -> const uint8_t * {
     if constexpr (PTRS)
-      row = pt.in[2 * j + h];
+      return pt.in[2 * j + h1];
     else
-      row = a.in_base + s * a.in_stripe_stride + (uint64_t)(2 * j + h) * a.in_row_stride;
-    uint32_t w[8];
-    load32(row + col, remain, w);
-    bit_transpose(w);
+      return a.in_base + s * a.in_stripe_stride + (uint64_t)(2 * j + h1) * a.in_row_stride;
+  };
+  auto prefetch = [&](uint64_t pair) {
+    const bool live = pair < total;
+    const uint32_t s = live ? (uint32_t)(pair / a.groups_per_stripe) : 0;
+    const uint64_t col = live ? (pair % a.groups_per_stripe) * 32 : 0;
+    const uint64_t remain = live ? a.len - col : 0;
 #pragma unroll
-    for (int b = 0; b < 8; b++) r[j][b] = w[b];
+    for (int j = 0; j < K / 2; j++) stage32(mine + j * kFftSlot, in_ptr(s, j) + col, remain);
+    cp_async_commit();
+  };
+
+  prefetch(pair0);
+  for (uint64_t rd = 0; rd < rounds; rd++) {
+    const uint64_t pair = pair0 + rd * stride;
+    const bool live = pair < total;
+    const uint32_t s = live ? (uint32_t)(pair / a.groups_per_stripe) : 0;
+    const uint64_t col = live ? (pair % a.groups_per_stripe) * 32 : 0;
+    const uint64_t remain = live ? a.len - col : 0;
+    cp_async_wait_all();
+    Reg r[K / 2];
+#pragma unroll
+    for (int j = 0; j < K / 2; j++) {
+      uint4 lo = *reinterpret_cast<const uint4 *>(mine + j * kFftSlot);
+      uint4 hi = *reinterpret_cast<const uint4 *>(mine + j * kFftSlot + kFftHalf);
+      uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+      bit_transpose(w);
+#pragma unroll
+      for (int b = 0; b < 8; b++) r[j][b] = w[b];
+    }
+    if (rd + 1 < rounds) prefetch(pair + stride);
+    constexpr int LG = log2k<K>();
+    // Interpolate: inverse transform on coset 0, levels 0 .. LG-1.
+    level0_pair<K, 0, true>(r, h0, h1);
+    levels_up<K, 1, 0, true>(r);
+    // Evaluate on coset K: forward transform, levels LG-1 .. 0.
+    levels_down<K, LG - 1, K, false>(r);
+    level0_pair<K, K, false>(r, h0, h1);
+    if (live) {
+#pragma unroll
+      for (int j = 0; j < K / 2; j++) {
+        uint8_t *row;
+        if constexpr (PTRS)
+          row = pt.out[2 * j + h1];
+        else
+          row = a.out_base + s * a.out_stripe_stride + (uint64_t)(2 * j + h1) * a.out_row_stride;
+        uint32_t w[8];
+#pragma unroll
+        for (int b = 0; b < 8; b++) w[b] = r[j][b];
+        bit_transpose(w);
+        store32(row + col, remain, w);
+      }
+    }
   }
-  constexpr int LG = log2k<K>();
-  // Interpolate: inverse transform on coset 0, levels 0 .. LG-1.
-  level0_pair<K, 0, true>(r, hmask);
-  levels_up<K, 1, 0, true>(r);
-  // Evaluate on coset K: forward transform, levels LG-1 .. 0.
-  levels_down<K, LG - 1, K, false>(r);
-  level0_pair<K, K, false>(r, hmask);
-  if (!live) return;
-#pragma unroll
-  for (int j = 0; j < K / 2; j++) {
-    uint8_t *row;
-    if constexpr (PTRS)
-      row = pt.out[2 * j + h];
-    else
-      row = a.out_base + s * a.out_stripe_stride + (uint64_t)(2 * j + h) * a.out_row_stride;
-    uint32_t w[8];
-#pragma unroll
-    for (int b = 0; b < 8; b++) w[b] = r[j][b];
-    bit_transpose(w);
-    store32(row + col, remain, w);
+}
+
+inline int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
   }
+  return n;
 }
 
 // Shapes with a bitsliced FFT kernel.
@@ -343,7 +409,14 @@ template <int K, bool PTRS>
 inline cudaError_t launch_fft_k(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
   uint64_t pairs = (uint64_t)a.n_stripes * a.groups_per_stripe;
   uint64_t blocks = (pairs * 2 + kFftThreads - 1) / kFftThreads;
-  fft_kk_kernel<K, PTRS><<<(unsigned)blocks, kFftThreads, 0, st>>>(a, pt);
+  blocks = std::min<uint64_t>(blocks, (uint64_t)sm_count() * kFftCtasPerSm);
+  const int smem = (K / 2) * kFftSlot;
+  auto kern = fft_kk_kernel<K, PTRS>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+  }
+  kern<<<(unsigned)blocks, kFftThreads, smem, st>>>(a, pt);
   return cudaGetLastError();
 }
 
