@@ -232,6 +232,10 @@ int rs_decode_rows(int field, size_t k, size_t m, const uint8_t *present, uint16
                    size_t out_len, size_t *n_rows);
 /* Number of this library's kernel launches so far in this process. */
 uint64_t rs_kernel_launch_count(void);
+/* Tuning hook (autotuner): launch shape of the bitsliced FFT kernel for batched calls,
+ * 0..rs_fft_variant_count()-1. Returns the previous value, or -1 if out of range. */
+int rs_set_fft_variant(int variant);
+int rs_fft_variant_count(void);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -187,19 +187,29 @@ __device__ __forceinline__ void level0_pair(Reg (&r)[K / 2], uint32_t h0, uint32
   });
 }
 
-template <int K, int L, int BETA, bool INV>
+// With SYNC the CTA meets at a barrier after every level, keeping the warps that
+// share a scheduler on the same stretch of straight-line code (one instruction
+// fetch then serves all of them).
+template <bool SYNC>
+__device__ __forceinline__ void phase_sync() {
+  if constexpr (SYNC) __syncthreads();
+}
+
+template <int K, int L, int BETA, bool INV, bool SYNC>
 __device__ __forceinline__ void levels_up(Reg (&r)[K / 2]) {  // L .. log2(K)-1
   if constexpr ((1 << L) < K) {
     level_local<K, L, BETA, INV>(r);
-    levels_up<K, L + 1, BETA, INV>(r);
+    phase_sync<SYNC>();
+    levels_up<K, L + 1, BETA, INV, SYNC>(r);
   }
 }
 
-template <int K, int L, int BETA, bool INV>
+template <int K, int L, int BETA, bool INV, bool SYNC>
 __device__ __forceinline__ void levels_down(Reg (&r)[K / 2]) {  // L .. 1
   if constexpr (L >= 1) {
     level_local<K, L, BETA, INV>(r);
-    levels_down<K, L - 1, BETA, INV>(r);
+    phase_sync<SYNC>();
+    levels_down<K, L - 1, BETA, INV, SYNC>(r);
   }
 }
 
@@ -266,6 +276,17 @@ __device__ __forceinline__ void store32(uint8_t *p, uint64_t remain, const uint3
   for (int t = 0; t < n; t++) p[t] = (uint8_t)(w[t >> 2] >> (8 * (t & 3)));
 }
 
+// One stripe of a ragged FFT batch: k data rows at in_base, k parity rows at out_base,
+// both row_stride apart; its 32-column groups start at group_begin in the flattened
+// group space (items sorted by group_begin).
+struct FftItem {
+  const uint8_t *in_base;
+  uint8_t *out_base;
+  uint64_t row_stride;
+  uint64_t len;
+  uint64_t group_begin;
+};
+
 struct FftArgs {
   const uint8_t *in_base;
   uint64_t in_row_stride, in_stripe_stride;
@@ -274,16 +295,68 @@ struct FftArgs {
   uint64_t len;
   uint32_t n_stripes;
   uint32_t groups_per_stripe;  // 32-column groups per stripe
+  // Ragged form (items != nullptr): per-stripe geometry, total_groups groups.
+  const FftItem *items;
+  uint32_t n_items;
+  uint64_t total_groups;
 };
 
-constexpr int kFftThreads = 128;
-constexpr int kFftCtasPerSm = 3;
+// Where one lane pair's 32-column group lives.
+struct FftLoc {
+  const uint8_t *in0;   // data row 0 (pointer-table form: unused)
+  uint8_t *out0;        // parity row 0
+  uint64_t in_rs, out_rs;
+  uint64_t col, remain;  // remain = 0 past the end
+};
+
+__device__ __forceinline__ FftLoc fft_locate(const FftArgs &a, uint64_t pair) {
+  FftLoc l{};
+  if (a.items) {
+    if (pair >= a.total_groups) return l;
+    uint32_t lo = 0, hi = a.n_items;
+    while (hi - lo > 1) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (a.items[mid].group_begin <= pair)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const FftItem &it = a.items[lo];
+    l.in0 = it.in_base;
+    l.out0 = it.out_base;
+    l.in_rs = l.out_rs = it.row_stride;
+    l.col = (pair - it.group_begin) * 32;
+    l.remain = it.len - l.col;
+    return l;
+  }
+  const uint64_t total = (uint64_t)a.n_stripes * a.groups_per_stripe;
+  if (pair >= total) return l;
+  const uint32_t s = (uint32_t)(pair / a.groups_per_stripe);
+  l.in0 = a.in_base + s * a.in_stripe_stride;
+  l.out0 = a.out_base + s * a.out_stripe_stride;
+  l.in_rs = a.in_row_stride;
+  l.out_rs = a.out_row_stride;
+  l.col = (pair % a.groups_per_stripe) * 32;
+  l.remain = a.len - l.col;
+  return l;
+}
+
+// Launch shapes of the FFT kernel: threads per CTA, CTAs per SM, and whether the CTA
+// meets at a barrier after every transform level (see phase_sync).
+struct FftVariant {
+  int threads, ctas, sync;
+};
+constexpr FftVariant kFftVariants[] = {{128, 3, 0}, {384, 1, 1}, {256, 1, 1}, {384, 1, 0}};
+constexpr int kFftVariantCount = sizeof(kFftVariants) / sizeof(kFftVariants[0]);
 
 // Per-thread staging of one 32-column group in shared memory: shard slot j, half q
-// (16 bytes each) of thread t sits at j*kFftSlot + q*kFftHalf + t*16, so a warp's
-// 16-byte accesses to one (j, q) are contiguous and free of bank conflicts.
-constexpr int kFftHalf = kFftThreads * 16;
-constexpr int kFftSlot = 2 * kFftHalf;
+// (16 bytes each) of thread t sits at j*slot + q*half + t*16 with half = 16*THREADS,
+// so a warp's 16-byte accesses to one (j, q) are contiguous and free of bank conflicts.
+template <int THREADS>
+struct FftStage {
+  static constexpr int kHalf = THREADS * 16;
+  static constexpr int kSlot = 2 * kHalf;
+};
 
 __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
   uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
@@ -294,77 +367,79 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Stage the 32 bytes at p (remain of them valid) into this thread's slot: two async
 // 16-byte copies when aligned and whole, else a zero-filled byte path.
+template <int HALF>
 __device__ __forceinline__ void stage32(uint8_t *slot, const uint8_t *p, uint64_t remain) {
   if (remain >= 32 && (((uintptr_t)p & 15u) == 0)) {
     cp_async16(slot, p);
-    cp_async16(slot + kFftHalf, p + 16);
+    cp_async16(slot + HALF, p + 16);
   } else {
     uint32_t w[8];
     load32(p, remain, w);
     *reinterpret_cast<uint4 *>(slot) = make_uint4(w[0], w[1], w[2], w[3]);
-    *reinterpret_cast<uint4 *>(slot + kFftHalf) = make_uint4(w[4], w[5], w[6], w[7]);
+    *reinterpret_cast<uint4 *>(slot + HALF) = make_uint4(w[4], w[5], w[6], w[7]);
   }
 }
 
 // Persistent lane pairs: round r handles group pair0 + r*stride of the flattened
 // (stripe, 32-column group) space. The next round's 32 bytes per shard are copied
 // into shared memory with cp.async while the current round computes. Every lane runs
-// every round (on zeros past the end) so each shuffle sees the full warp.
-template <int K, bool PTRS>
-__global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm)
+// every round (on zeros past the end) so each shuffle sees the full warp and every
+// barrier sees the full CTA.
+template <int K, bool PTRS, int THREADS, int CTAS, bool SYNC>
+__global__ void __launch_bounds__(THREADS, CTAS)
     fft_kk_kernel(const FftArgs a, const __grid_constant__ PtrTableT<PTRS> pt) {
   extern __shared__ __align__(16) uint8_t stage[];
   using namespace fftc;
+  using St = FftStage<THREADS>;
   const uint32_t tid = threadIdx.x;
   const uint32_t h1 = tid & 1, h0 = 1 - h1;
-  const uint64_t total = (uint64_t)a.n_stripes * a.groups_per_stripe;
-  const uint64_t stride = (uint64_t)gridDim.x * (kFftThreads / 2);
+  const uint64_t total = a.items ? a.total_groups : (uint64_t)a.n_stripes * a.groups_per_stripe;
+  const uint64_t stride = (uint64_t)gridDim.x * (THREADS / 2);
   const uint64_t rounds = (total + stride - 1) / stride;
-  const uint64_t pair0 = ((uint64_t)blockIdx.x * kFftThreads + tid) >> 1;
+  const uint64_t pair0 = ((uint64_t)blockIdx.x * THREADS + tid) >> 1;
   uint8_t *mine = stage + tid * 16;
 
-  auto in_ptr = [&](uint32_t s, int j) -> const uint8_t * {
+  auto in_ptr = [&](const FftLoc &l, int j) -> const uint8_t * {
     if constexpr (PTRS)
       return pt.in[2 * j + h1];
     else
-      return a.in_base + s * a.in_stripe_stride + (uint64_t)(2 * j + h1) * a.in_row_stride;
+      return l.in0 + (uint64_t)(2 * j + h1) * l.in_rs;
   };
   auto prefetch = [&](uint64_t pair) {
-    const bool live = pair < total;
-    const uint32_t s = live ? (uint32_t)(pair / a.groups_per_stripe) : 0;
-    const uint64_t col = live ? (pair % a.groups_per_stripe) * 32 : 0;
-    const uint64_t remain = live ? a.len - col : 0;
+    const FftLoc l = fft_locate(a, pair);
 #pragma unroll
-    for (int j = 0; j < K / 2; j++) stage32(mine + j * kFftSlot, in_ptr(s, j) + col, remain);
+    for (int j = 0; j < K / 2; j++) stage32<St::kHalf>(mine + j * St::kSlot, in_ptr(l, j) + l.col, l.remain);
     cp_async_commit();
   };
 
   prefetch(pair0);
   for (uint64_t rd = 0; rd < rounds; rd++) {
     const uint64_t pair = pair0 + rd * stride;
-    const bool live = pair < total;
-    const uint32_t s = live ? (uint32_t)(pair / a.groups_per_stripe) : 0;
-    const uint64_t col = live ? (pair % a.groups_per_stripe) * 32 : 0;
-    const uint64_t remain = live ? a.len - col : 0;
+    const FftLoc loc = fft_locate(a, pair);
+    const bool live = loc.remain != 0;
+    const uint64_t col = loc.col, remain = loc.remain;
     cp_async_wait_all();
     Reg r[K / 2];
 #pragma unroll
     for (int j = 0; j < K / 2; j++) {
-      uint4 lo = *reinterpret_cast<const uint4 *>(mine + j * kFftSlot);
-      uint4 hi = *reinterpret_cast<const uint4 *>(mine + j * kFftSlot + kFftHalf);
+      uint4 lo = *reinterpret_cast<const uint4 *>(mine + j * St::kSlot);
+      uint4 hi = *reinterpret_cast<const uint4 *>(mine + j * St::kSlot + St::kHalf);
       uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
       bit_transpose(w);
 #pragma unroll
       for (int b = 0; b < 8; b++) r[j][b] = w[b];
     }
     if (rd + 1 < rounds) prefetch(pair + stride);
+    phase_sync<SYNC>();
     constexpr int LG = log2k<K>();
     // Interpolate: inverse transform on coset 0, levels 0 .. LG-1.
     level0_pair<K, 0, true>(r, h0, h1);
-    levels_up<K, 1, 0, true>(r);
+    phase_sync<SYNC>();
+    levels_up<K, 1, 0, true, SYNC>(r);
     // Evaluate on coset K: forward transform, levels LG-1 .. 0.
-    levels_down<K, LG - 1, K, false>(r);
+    levels_down<K, LG - 1, K, false, SYNC>(r);
     level0_pair<K, K, false>(r, h0, h1);
+    phase_sync<SYNC>();
     if (live) {
 #pragma unroll
       for (int j = 0; j < K / 2; j++) {
@@ -372,7 +447,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm)
         if constexpr (PTRS)
           row = pt.out[2 * j + h1];
         else
-          row = a.out_base + s * a.out_stripe_stride + (uint64_t)(2 * j + h1) * a.out_row_stride;
+          row = loc.out0 + (uint64_t)(2 * j + h1) * loc.out_rs;
         uint32_t w[8];
 #pragma unroll
         for (int b = 0; b < 8; b++) w[b] = r[j][b];
@@ -380,7 +455,14 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm)
         store32(row + col, remain, w);
       }
     }
+    phase_sync<SYNC>();
   }
+}
+
+// Selected launch shape (index into kFftVariants); set by rs_set_fft_variant.
+inline int &fft_variant() {
+  static int v = 1;
+  return v;
 }
 
 inline int sm_count() {
@@ -405,25 +487,37 @@ inline const FftShape *find_fft_shape(size_t k, size_t m) {
   return nullptr;
 }
 
-template <int K, bool PTRS>
-inline cudaError_t launch_fft_k(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
-  uint64_t pairs = (uint64_t)a.n_stripes * a.groups_per_stripe;
-  uint64_t blocks = (pairs * 2 + kFftThreads - 1) / kFftThreads;
-  blocks = std::min<uint64_t>(blocks, (uint64_t)sm_count() * kFftCtasPerSm);
-  const int smem = (K / 2) * kFftSlot;
-  auto kern = fft_kk_kernel<K, PTRS>;
+template <int K, bool PTRS, int V>
+inline cudaError_t launch_fft_kv(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
+  constexpr FftVariant var = kFftVariants[V];
+  uint64_t pairs = a.items ? a.total_groups : (uint64_t)a.n_stripes * a.groups_per_stripe;
+  uint64_t blocks = (pairs * 2 + var.threads - 1) / var.threads;
+  blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, (uint64_t)sm_count() * var.ctas));
+  const int smem = (K / 2) * FftStage<var.threads>::kSlot;
+  auto kern = fft_kk_kernel<K, PTRS, var.threads, var.ctas, (bool)var.sync>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
   }
-  kern<<<(unsigned)blocks, kFftThreads, smem, st>>>(a, pt);
+  kern<<<(unsigned)blocks, var.threads, smem, st>>>(a, pt);
   return cudaGetLastError();
+}
+
+template <int K, bool PTRS>
+inline cudaError_t launch_fft_k(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
+  if constexpr (PTRS) return launch_fft_kv<K, PTRS, 1>(a, pt, st);  // single-stripe calls
+  switch (fft_variant()) {
+    case 0: return launch_fft_kv<K, PTRS, 0>(a, pt, st);
+    case 2: return launch_fft_kv<K, PTRS, 2>(a, pt, st);
+    case 3: return launch_fft_kv<K, PTRS, 3>(a, pt, st);
+    default: return launch_fft_kv<K, PTRS, 1>(a, pt, st);
+  }
 }
 
 template <bool PTRS>
 inline int launch_fft_any(const FftShape &sh, const FftArgs &a, const PtrTableT<PTRS> &pt,
                           cudaStream_t st) {
-  if (a.len == 0 || a.n_stripes == 0) return RS_OK;
+  if (a.items ? a.total_groups == 0 : (a.len == 0 || a.n_stripes == 0)) return RS_OK;
   cudaError_t e;
   switch (sh.k) {
     case 2: e = launch_fft_k<2, PTRS>(a, pt, st); break;
@@ -454,6 +548,17 @@ inline int launch_fft8(const FftShape &sh, const uint8_t *in_base, uint64_t in_r
   a.len = len;
   a.n_stripes = n_stripes;
   a.groups_per_stripe = (uint32_t)((len + 31) / 32);
+  PtrTableT<false> pt{};
+  return launch_fft_any<false>(sh, a, pt, st);
+}
+
+// Ragged batch of (K, K) stripes described by a device item array.
+inline int launch_fft8_items(const FftShape &sh, const FftItem *d_items, uint32_t n_items,
+                             uint64_t total_groups, cudaStream_t st) {
+  FftArgs a{};
+  a.items = d_items;
+  a.n_items = n_items;
+  a.total_groups = total_groups;
   PtrTableT<false> pt{};
   return launch_fft_any<false>(sh, a, pt, st);
 }

@@ -13,6 +13,7 @@
 #include "kernels_matrix.cuh"
 #include "kernels_fft.cuh"
 #include "kernels_plan.cuh"
+#include "codec8.hpp"
 
 namespace rsb {
 
@@ -86,7 +87,7 @@ static int launch_gf8_t(const ApplyArgs &a, const PtrTableT<PTRS> &pt, cudaStrea
   return RS_OK;
 }
 
-static int launch_gf8(const ApplyArgs &a, const PtrTable *pt, bool verify, cudaStream_t st) {
+int launch_gf8(const ApplyArgs &a, const PtrTable *pt, bool verify, cudaStream_t st) {
   if (a.len == 0 || a.rows == 0 || a.n_stripes == 0) return RS_OK;
   if (pt) {
     PtrTableT<true> t;
@@ -102,50 +103,17 @@ static int launch_gf8(const ApplyArgs &a, const PtrTable *pt, bool verify, cudaS
 // GF(2^8) codec
 // ------------------------------------------------------------------------------
 
-struct Gen8 {
-  int device = 0;
-  size_t k = 0, m = 0;
-  std::vector<uint8_t> rows;  // m x k
-  uint8_t *d_rows = nullptr;
-  const FftShape *fft = nullptr;  // bitsliced FFT program for this shape, if any
-  ~Gen8() {
-    if (d_rows) {
-      cudaSetDevice(device);
-      cudaFree(d_rows);
-    }
-  }
-};
-
-}  // namespace rsb
-
-using namespace rsb;
-
-struct rs8_codec {
-  std::shared_ptr<const Gen8> gen;
-  std::shared_ptr<PlanCache> plans;
-  std::shared_ptr<Exec> exec;
-  std::atomic<int> route{0};
-};
-
-struct rs8_decoder {
-  std::shared_ptr<const Gen8> gen;
-  std::shared_ptr<const Plan> plan;
-  std::shared_ptr<Exec> exec;
-};
-
-namespace rsb {
-
 // Encode route for a shape and length: the bitsliced FFT kernel where the shape has
 // a program and the shard holds at least one full 32-column group per thread pair,
 // else the matrix kernel.
-static bool use_fft8(const rs8_codec *c, size_t len) {
+bool use_fft8(const rs8_codec *c, size_t len) {
   int r = c->route.load();
   if (r == 1 || !c->gen->fft) return false;
   if (r == 2) return true;
   return len >= 64;
 }
 
-static int encode8_strided(rs8_codec *c, const uint8_t *in_base, uint64_t in_row, uint64_t in_stripe,
+int encode8_strided(rs8_codec *c, const uint8_t *in_base, uint64_t in_row, uint64_t in_stripe,
                            uint8_t *out_base, uint64_t out_row, uint64_t out_stripe, size_t n_stripes,
                            size_t len, cudaStream_t st) {
   const Gen8 &g = *c->gen;
@@ -288,6 +256,8 @@ static int check_equal_lengths(const size_t n, size_t len) {
 // Exported entry points
 // ==============================================================================
 
+using namespace rsb;
+
 extern "C" {
 
 const char *rs_strerror(int status) {
@@ -322,6 +292,15 @@ uint32_t rs_abi_version(void) { return (1u << 16) | 0u; }
 int rs_device_check(void) { return ensure_device(nullptr); }
 
 uint64_t rs_kernel_launch_count(void) { return g_launches.load(); }
+
+int rs_set_fft_variant(int variant) {
+  if (variant < 0 || variant >= kFftVariantCount) return -1;
+  int old = fft_variant();
+  fft_variant() = variant;
+  return old;
+}
+
+int rs_fft_variant_count(void) { return kFftVariantCount; }
 
 int rs_generator_rows(int field, size_t k, size_t m, uint16_t *out, size_t out_len) {
   if (!out || (field != 8 && field != 16)) return RS_ERR_INVALID_ARGUMENT;
