@@ -161,6 +161,41 @@ int rs8_reconstruct_batch_dev(rs8_t *codec, uint8_t *d_rows, size_t stripe_strid
                               size_t n_stripes, size_t row_len, const uint8_t *present,
                               int data_only, int *statuses, void *stream);
 
+/* ---- mixed batches: stripes of any GF(2^8) shapes, lengths and erasure patterns ----
+ * No counterpart in the reference (it codes one stripe per call on one core). A batch
+ * is validated and planned once: decode matrices for every reconstruct item are built
+ * on the device in one launch per shape, the work is grouped by route (bitsliced FFT
+ * per (K,K) shape, one ragged matrix launch for the rest) and captured into a CUDA
+ * graph; rs_batch_launch replays it. Each item's status is the reference error its
+ * single-stripe call would return (0 = Ok); failed items are left out of the graph. */
+enum rs_batch_op {
+  RS_BATCH_ENCODE = 0,           /* rows [0,k) -> rows [k,n) */
+  RS_BATCH_RECONSTRUCT = 1,      /* rebuild every absent row */
+  RS_BATCH_RECONSTRUCT_DATA = 2  /* rebuild absent data rows only */
+};
+enum rs_batch_flags {
+  RS_BATCH_MATRIX_ONLY = 1, /* the plain route for every item (comparison baseline) */
+  RS_BATCH_NO_GRAPH = 2     /* launch kernels directly instead of through a graph */
+};
+typedef struct {
+  rs8_t *codec;           /* the stripe's shape (k, m) */
+  uint8_t *d_rows;        /* n = k+m rows of row_len bytes, row_stride apart (device) */
+  size_t row_stride;
+  size_t row_len;
+  int op;                 /* enum rs_batch_op */
+  const uint8_t *present; /* n flags (host memory), reconstruct ops only */
+} rs_batch_item;
+typedef struct rs_batch rs_batch_t;
+int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *statuses,
+                    rs_batch_t **out);
+/* Enqueues one replay of the batch on `stream`. */
+int rs_batch_launch(rs_batch_t *batch, void *stream);
+/* Kernel launches per replay, stripes on each route, algorithmic bytes per replay
+ * ((k+m)*len per encode, (k+e)*len per reconstruct rebuilding e rows). */
+int rs_batch_stats(const rs_batch_t *batch, size_t *launches, size_t *fft_items,
+                   size_t *matrix_items, uint64_t *bytes);
+void rs_batch_free(rs_batch_t *batch);
+
 /* ========================= ReedSolomon16 (GF((2^8)^2)) ========================= */
 
 /* ReedSolomon16::new, src/reedsolomon16.rs:281-319 (k + m <= 65536). */

@@ -4,7 +4,13 @@ The directory name contains a hyphen, so import it through `load_package()` in
 `__graft_entry__` (or tests/conftest.py), which registers it as `reed_solomon_b200`.
 """
 from .coder import (  # noqa: F401
+    ENCODE,
     ERROR_NAMES,
+    MATRIX_ONLY,
+    NO_GRAPH,
+    RECONSTRUCT,
+    RECONSTRUCT_DATA,
+    Batch,
     PreparedDecoder,
     PreparedDecoder16,
     ReedSolomon,

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "librsb200.so")
-SOURCES = ["rs_abi.cu", "rs16_abi.cu"]
+SOURCES = ["rs_abi.cu", "rs16_abi.cu", "rs_batch.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 FLAGS = [

@@ -407,6 +407,58 @@ class PreparedDecoder16(_Prepared):
     _fn = "rs16"
 
 
+class _BatchItem(ctypes.Structure):
+    _fields_ = [("codec", ctypes.c_void_p), ("d_rows", ctypes.c_void_p), ("row_stride", ctypes.c_size_t),
+                ("row_len", ctypes.c_size_t), ("op", ctypes.c_int), ("present", ctypes.POINTER(ctypes.c_uint8))]
+
+
+ENCODE, RECONSTRUCT, RECONSTRUCT_DATA = 0, 1, 2
+MATRIX_ONLY, NO_GRAPH = 1, 2
+
+
+class Batch:
+    """A mixed batch of GF(2^8) stripes (rs_batch_create): items are tuples
+    (codec, rows, row_stride, row_len, op, present) with `rows` a CUDA tensor or device
+    pointer holding n = k+m rows; `present` (n flags) for reconstruct ops."""
+
+    def __init__(self, items, flags=0):
+        self._L = _lib.load()
+        n = len(items)
+        arr = (_BatchItem * max(n, 1))()
+        self._keep = []
+        for i, (codec, rows, stride, row_len, op, present) in enumerate(items):
+            arr[i].codec = codec._h.value
+            arr[i].d_rows = _dev_ptr(rows)
+            arr[i].row_stride = stride
+            arr[i].row_len = row_len
+            arr[i].op = op
+            if present is not None:
+                f, fp = _flags(present)
+                self._keep.append(f)
+                arr[i].present = fp
+        self._codecs = [it[0] for it in items]
+        st = (ctypes.c_int * max(n, 1))()
+        h = ctypes.c_void_p()
+        _check(self._L.rs_batch_create(arr, n, flags, st, ctypes.byref(h)))
+        self._h = h
+        self.statuses = list(st)[:n]
+
+    def launch(self, stream=0):
+        _check(self._L.rs_batch_launch(self._h, stream))
+
+    def stats(self):
+        la, fi, mi = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_size_t()
+        by = ctypes.c_uint64()
+        _check(self._L.rs_batch_stats(self._h, ctypes.byref(la), ctypes.byref(fi), ctypes.byref(mi), ctypes.byref(by)))
+        return {"launches": la.value, "fft_items": fi.value, "matrix_items": mi.value, "bytes": by.value}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._L.rs_batch_free(h)
+            self._h = None
+
+
 # gf::mul_slice / mul_slice_xor, src/gf/mod.rs:69-85
 def mul_slice(out, inp, c):
     o = _as_u8(out, True)

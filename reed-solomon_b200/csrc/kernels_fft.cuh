@@ -346,7 +346,8 @@ __device__ __forceinline__ FftLoc fft_locate(const FftArgs &a, uint64_t pair) {
 struct FftVariant {
   int threads, ctas, sync;
 };
-constexpr FftVariant kFftVariants[] = {{128, 3, 0}, {384, 1, 1}, {256, 1, 1}, {384, 1, 0}};
+constexpr FftVariant kFftVariants[] = {{128, 3, 0}, {384, 1, 1}, {256, 1, 1}, {384, 1, 0},
+                                       {128, 4, 0}, {128, 6, 0}};
 constexpr int kFftVariantCount = sizeof(kFftVariants) / sizeof(kFftVariants[0]);
 
 // Per-thread staging of one 32-column group in shared memory: shard slot j, half q
@@ -510,6 +511,8 @@ inline cudaError_t launch_fft_k(const FftArgs &a, const PtrTableT<PTRS> &pt, cud
     case 0: return launch_fft_kv<K, PTRS, 0>(a, pt, st);
     case 2: return launch_fft_kv<K, PTRS, 2>(a, pt, st);
     case 3: return launch_fft_kv<K, PTRS, 3>(a, pt, st);
+    case 4: return launch_fft_kv<K, PTRS, 4>(a, pt, st);
+    case 5: return launch_fft_kv<K, PTRS, 5>(a, pt, st);
     default: return launch_fft_kv<K, PTRS, 1>(a, pt, st);
   }
 }
