@@ -271,6 +271,10 @@ uint64_t rs_kernel_launch_count(void);
  * 0..rs_fft_variant_count()-1. Returns the previous value, or -1 if out of range. */
 int rs_set_fft_variant(int variant);
 int rs_fft_variant_count(void);
+/* Tuning hook: lane-group width of the (k,k) FFT kernel, 0 = narrow, 1 = wide (more
+ * lanes per 32-column group, fewer registers per lane). Returns the previous value,
+ * or -1 when (k,k) has no FFT kernel. */
+int rs_set_fft_lanes(size_t k, int wide);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

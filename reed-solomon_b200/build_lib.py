@@ -10,7 +10,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "librsb200.so")
-SOURCES = ["rs_abi.cu", "rs16_abi.cu", "rs_batch.cu"]
+SOURCES = ["rs_abi.cu", "rs16_abi.cu", "rs_batch.cu", "fft_k_small.cu", "fft_k16.cu", "fft_k32.cu",
+           "fft_k64.cu", "fft_k128.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 FLAGS = [
@@ -35,15 +36,27 @@ def stale():
 def build(force=False, verbose=False):
     if not force and not stale():
         return OUT
-    objs = []
+    from concurrent.futures import ThreadPoolExecutor
+
     build_dir = os.path.join(HERE, "_build")
     os.makedirs(build_dir, exist_ok=True)
     extra = ["-Xptxas", "-v"] if verbose else []
-    for src in SOURCES:
-        obj = os.path.join(build_dir, src.replace(".cu", ".o"))
-        cmd = [NVCC, *FLAGS, *extra, "-DRSB_BUILDING_LIBRARY", "-c", os.path.join(CSRC, src), "-o", obj]
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+    objs = [os.path.join(build_dir, src.replace(".cu", ".o")) for src in SOURCES]
+
+    def compile_one(i):
+        cmd = [NVCC, *FLAGS, *extra, "-c", os.path.join(CSRC, SOURCES[i]), "-o", objs[i]]
+        return subprocess.run(cmd, capture_output=True, text=True)
+
+    # Largest translation units first; one nvcc per core.
+    order = sorted(range(len(SOURCES)), key=lambda i: -os.path.getsize(os.path.join(CSRC, SOURCES[i])))
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+        results = dict(zip(order, ex.map(compile_one, order)))
+    for i in range(len(SOURCES)):
+        r = results[i]
+        if verbose or r.returncode:
+            sys.stderr.write(r.stdout + r.stderr)
+        if r.returncode:
+            raise subprocess.CalledProcessError(r.returncode, "nvcc " + SOURCES[i])
     tmp = OUT + ".tmp"
     subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp, *objs,
                     "-Xcompiler", "-fPIC"], check=True)

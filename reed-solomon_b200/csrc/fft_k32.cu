@@ -1,0 +1,8 @@
+// Instantiates the bitsliced FFT encode kernels for (K,K) with K = 32 (kernels_fft.cuh).
+#include "kernels_fft.cuh"
+
+namespace rsb {
+
+RSB_FFT_DEFINE(32)
+
+}  // namespace rsb

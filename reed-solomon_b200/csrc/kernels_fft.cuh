@@ -127,34 +127,62 @@ __device__ __forceinline__ void butterfly(Reg &lo, Reg &hi) {
   if constexpr (!INV) xor_into(hi, lo);
 }
 
-// Lane-local level L >= 1 of a K-point transform on coset BETA; r[j] is register 2j+h.
-template <int K, int L, int BETA, bool INV>
-__device__ __forceinline__ void level_local(Reg (&r)[K / 2]) {
-  constexpr int S = 1 << L;
-  static_for<0, K / 2>([&](auto jj) {
+// Lane groups. A group of G = 2^W lanes shares one 32-column group; lane q holds
+// program registers i = (j << W) | q in its slots j = 0 .. K/G - 1.
+//
+// Level L >= W pairs slots j and j + 2^(L-W) within each lane; the butterfly's block
+// base has only bits >= W, so its constant is the same in every lane.
+template <int K, int W, int L, int BETA, bool INV>
+__device__ __forceinline__ void level_local(Reg (&r)[K >> W]) {
+  constexpr int SJ = 1 << (L - W);  // slot stride
+  static_for<0, (K >> W)>([&](auto jj) {
     constexpr int j = decltype(jj)::value;
-    constexpr int i = 2 * j;
-    if constexpr (((i >> L) & 1) == 0) {
-      constexpr int base = i & ~(2 * S - 1);
+    if constexpr (((j / SJ) & 1) == 0) {
+      constexpr int base = (j << W) & ~((2 << L) - 1);
       constexpr uint8_t c = kWhat.v[L][BETA ^ base];
-      butterfly<c, INV>(r[j], r[j + S / 2]);
+      butterfly<c, INV>(r[j], r[j + SJ]);
     }
   });
 }
 
-// Level 0 across the lane pair; h1 is 0 on lane 0 (even registers) and 1 on lane 1,
-// h0 = 1 - h1. Lane selects are written as integer multiply-adds by 0/1 so they issue
-// on the FMA pipe, which the LOP3-heavy butterflies leave idle.
-template <int K, int BETA, bool INV>
-__device__ __forceinline__ void level0_pair(Reg (&r)[K / 2], uint32_t h0, uint32_t h1) {
-  static_for<0, K / 2>([&](auto jj) {
+// d ^= mask & (E * s), mask all-ones or zero (a lane-bit select).
+template <uint8_t E>
+__device__ __forceinline__ void masked_mul_acc(Reg &d, const Reg &s, uint32_t mask) {
+  if constexpr (E != 0) {
+    Reg t;
+    mul_set<E>(t, s);
+#pragma unroll
+    for (int b = 0; b < 8; b++) d[b] ^= t[b] & mask;
+  }
+}
+
+// The lane-dependent part of a cross-lane constant at level L. The block base of
+// register (j << W) | q is (j << W) | (q with bits <= L cleared); WHAT[L] is GF(2)-linear,
+// so the constant is WHAT[L][BETA ^ (j << W)] plus WHAT[L][2^t] for every lane bit t
+// in (L, W) that is set in q. qm[t] is all-ones when bit t of q is set.
+template <int W, int L, int T>
+__device__ __forceinline__ void lane_terms(Reg &d, const Reg &s, const uint32_t (&qm)[8]) {
+  if constexpr (T < W) {
+    masked_mul_acc<kWhat.v[L][1 << T]>(d, s, qm[T]);
+    lane_terms<W, L, T + 1>(d, s, qm);
+  }
+}
+
+// Level L < W: the butterfly pairs lanes q and q ^ 2^L. Each lane swaps its register
+// with one shuffle per plane and keeps its own half; h1 = bit L of q (1 on the lane
+// owning the upper register), h0 = 1 - h1. Lane selects are integer multiply-adds by
+// 0/1 so they issue on the FMA pipe, which the LOP3-heavy butterflies leave idle.
+template <int K, int W, int L, int BETA, bool INV>
+__device__ __forceinline__ void level_cross(Reg (&r)[K >> W], uint32_t q, const uint32_t (&qm)[8]) {
+  const uint32_t h1 = (q >> L) & 1, h0 = 1 - h1;
+  static_for<0, (K >> W)>([&](auto jj) {
     constexpr int j = decltype(jj)::value;
-    constexpr uint8_t c = kWhat.v[0][BETA ^ (2 * j)];
+    constexpr uint8_t c = kWhat.v[L][BETA ^ (j << W)];
     Reg p;
 #pragma unroll
-    for (int b = 0; b < 8; b++) p[b] = __shfl_xor_sync(0xffffffffu, r[j][b], 1);
+    for (int b = 0; b < 8; b++) p[b] = __shfl_xor_sync(0xffffffffu, r[j][b], 1 << L);
     if constexpr (INV) {
-      // hi' = lo ^ hi; lo' = lo ^ c*hi'. Lane 0 owns lo, lane 1 owns hi.
+      // hi' = lo ^ hi; lo' = lo ^ c*hi'.
       Reg t, v;
 #pragma unroll
       for (int b = 0; b < 8; b++) {
@@ -165,10 +193,11 @@ __device__ __forceinline__ void level0_pair(Reg (&r)[K / 2], uint32_t h0, uint32
         xor_into(v, t);
       else if constexpr (c != 0)
         mul_acc<c>(v, t);
+      lane_terms<W, L, L + 1>(v, t, qm);
 #pragma unroll
       for (int b = 0; b < 8; b++) r[j][b] = t[b] * h1 + v[b] * h0;
     } else {
-      // lo' = lo ^ c*hi; hi' = hi ^ lo'. Lane 0: own ^ c*p; lane 1: own ^ p ^ c*own.
+      // lo' = lo ^ c*hi; hi' = hi ^ lo'. Lower lane: own ^ c*p; upper: own ^ p ^ c*own.
       Reg z, u;
 #pragma unroll
       for (int b = 0; b < 8; b++) z[b] = r[j][b] * h1 + p[b] * h0;
@@ -181,6 +210,7 @@ __device__ __forceinline__ void level0_pair(Reg (&r)[K / 2], uint32_t h0, uint32
 #pragma unroll
         for (int b = 0; b < 8; b++) u[b] = 0;
       }
+      lane_terms<W, L, L + 1>(u, z, qm);
 #pragma unroll
       for (int b = 0; b < 8; b++) r[j][b] ^= u[b] ^ (p[b] * h1);
     }
@@ -188,28 +218,36 @@ __device__ __forceinline__ void level0_pair(Reg (&r)[K / 2], uint32_t h0, uint32
 }
 
 // With SYNC the CTA meets at a barrier after every level, keeping the warps that
-// share a scheduler on the same stretch of straight-line code (one instruction
-// fetch then serves all of them).
+// share a scheduler on the same stretch of straight-line code.
 template <bool SYNC>
 __device__ __forceinline__ void phase_sync() {
   if constexpr (SYNC) __syncthreads();
 }
 
-template <int K, int L, int BETA, bool INV, bool SYNC>
-__device__ __forceinline__ void levels_up(Reg (&r)[K / 2]) {  // L .. log2(K)-1
+template <int K, int W, int L, int BETA, bool INV, bool SYNC>
+__device__ __forceinline__ void level_any(Reg (&r)[K >> W], uint32_t q, const uint32_t (&qm)[8]) {
+  if constexpr (L < W)
+    level_cross<K, W, L, BETA, INV>(r, q, qm);
+  else
+    level_local<K, W, L, BETA, INV>(r);
+  phase_sync<SYNC>();
+}
+
+// Inverse transform: levels L .. log2(K)-1 ascending.
+template <int K, int W, int L, int BETA, bool SYNC>
+__device__ __forceinline__ void levels_up(Reg (&r)[K >> W], uint32_t q, const uint32_t (&qm)[8]) {
   if constexpr ((1 << L) < K) {
-    level_local<K, L, BETA, INV>(r);
-    phase_sync<SYNC>();
-    levels_up<K, L + 1, BETA, INV, SYNC>(r);
+    level_any<K, W, L, BETA, true, SYNC>(r, q, qm);
+    levels_up<K, W, L + 1, BETA, SYNC>(r, q, qm);
   }
 }
 
-template <int K, int L, int BETA, bool INV, bool SYNC>
-__device__ __forceinline__ void levels_down(Reg (&r)[K / 2]) {  // L .. 1
-  if constexpr (L >= 1) {
-    level_local<K, L, BETA, INV>(r);
-    phase_sync<SYNC>();
-    levels_down<K, L - 1, BETA, INV, SYNC>(r);
+// Forward transform: levels L .. 0 descending.
+template <int K, int W, int L, int BETA, bool SYNC>
+__device__ __forceinline__ void levels_down(Reg (&r)[K >> W], uint32_t q, const uint32_t (&qm)[8]) {
+  if constexpr (L >= 0) {
+    level_any<K, W, L, BETA, false, SYNC>(r, q, qm);
+    levels_down<K, W, L - 1, BETA, SYNC>(r, q, qm);
   }
 }
 
@@ -346,8 +384,7 @@ __device__ __forceinline__ FftLoc fft_locate(const FftArgs &a, uint64_t pair) {
 struct FftVariant {
   int threads, ctas, sync;
 };
-constexpr FftVariant kFftVariants[] = {{128, 3, 0}, {384, 1, 1}, {256, 1, 1}, {384, 1, 0},
-                                       {128, 4, 0}, {128, 6, 0}};
+constexpr FftVariant kFftVariants[] = {{128, 3, 0}, {128, 4, 0}};
 constexpr int kFftVariantCount = sizeof(kFftVariants) / sizeof(kFftVariants[0]);
 
 // Per-thread staging of one 32-column group in shared memory: shard slot j, half q
@@ -381,48 +418,52 @@ __device__ __forceinline__ void stage32(uint8_t *slot, const uint8_t *p, uint64_
   }
 }
 
-// Persistent lane pairs: round r handles group pair0 + r*stride of the flattened
-// (stripe, 32-column group) space. The next round's 32 bytes per shard are copied
-// into shared memory with cp.async while the current round computes. Every lane runs
-// every round (on zeros past the end) so each shuffle sees the full warp and every
-// barrier sees the full CTA.
-template <int K, bool PTRS, int THREADS, int CTAS, bool SYNC>
+// Persistent lane groups: round r handles 32-column group grp0 + r*stride of the
+// flattened (stripe, group) space; lane q of a group of 2^W lanes holds registers
+// (j << W) | q. The next round's 32 bytes per shard are copied into shared memory with
+// cp.async while the current round computes. Every lane runs every round (on zeros
+// past the end) so each shuffle sees the full warp and every barrier the full CTA.
+template <int K, int W, bool PTRS, int THREADS, int CTAS, bool SYNC>
 __global__ void __launch_bounds__(THREADS, CTAS)
     fft_kk_kernel(const FftArgs a, const __grid_constant__ PtrTableT<PTRS> pt) {
   extern __shared__ __align__(16) uint8_t stage[];
   using namespace fftc;
   using St = FftStage<THREADS>;
+  constexpr int S = K >> W;  // slots per lane
   const uint32_t tid = threadIdx.x;
-  const uint32_t h1 = tid & 1, h0 = 1 - h1;
+  const uint32_t q = tid & ((1u << W) - 1);
+  uint32_t qm[8];
+#pragma unroll
+  for (int t = 0; t < 8; t++) qm[t] = ((q >> t) & 1) ? 0xffffffffu : 0u;
   const uint64_t total = a.items ? a.total_groups : (uint64_t)a.n_stripes * a.groups_per_stripe;
-  const uint64_t stride = (uint64_t)gridDim.x * (THREADS / 2);
+  const uint64_t stride = (uint64_t)gridDim.x * (THREADS >> W);
   const uint64_t rounds = (total + stride - 1) / stride;
-  const uint64_t pair0 = ((uint64_t)blockIdx.x * THREADS + tid) >> 1;
+  const uint64_t grp0 = ((uint64_t)blockIdx.x * THREADS + tid) >> W;
   uint8_t *mine = stage + tid * 16;
 
   auto in_ptr = [&](const FftLoc &l, int j) -> const uint8_t * {
     if constexpr (PTRS)
-      return pt.in[2 * j + h1];
+      return pt.in[(j << W) | q];
     else
-      return l.in0 + (uint64_t)(2 * j + h1) * l.in_rs;
+      return l.in0 + (uint64_t)((j << W) | q) * l.in_rs;
   };
-  auto prefetch = [&](uint64_t pair) {
-    const FftLoc l = fft_locate(a, pair);
+  auto prefetch = [&](uint64_t grp) {
+    const FftLoc l = fft_locate(a, grp);
 #pragma unroll
-    for (int j = 0; j < K / 2; j++) stage32<St::kHalf>(mine + j * St::kSlot, in_ptr(l, j) + l.col, l.remain);
+    for (int j = 0; j < S; j++) stage32<St::kHalf>(mine + j * St::kSlot, in_ptr(l, j) + l.col, l.remain);
     cp_async_commit();
   };
 
-  prefetch(pair0);
+  prefetch(grp0);
   for (uint64_t rd = 0; rd < rounds; rd++) {
-    const uint64_t pair = pair0 + rd * stride;
-    const FftLoc loc = fft_locate(a, pair);
+    const uint64_t grp = grp0 + rd * stride;
+    const FftLoc loc = fft_locate(a, grp);
     const bool live = loc.remain != 0;
     const uint64_t col = loc.col, remain = loc.remain;
     cp_async_wait_all();
-    Reg r[K / 2];
+    Reg r[S];
 #pragma unroll
-    for (int j = 0; j < K / 2; j++) {
+    for (int j = 0; j < S; j++) {
       uint4 lo = *reinterpret_cast<const uint4 *>(mine + j * St::kSlot);
       uint4 hi = *reinterpret_cast<const uint4 *>(mine + j * St::kSlot + St::kHalf);
       uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
@@ -430,25 +471,21 @@ __global__ void __launch_bounds__(THREADS, CTAS)
 #pragma unroll
       for (int b = 0; b < 8; b++) r[j][b] = w[b];
     }
-    if (rd + 1 < rounds) prefetch(pair + stride);
+    if (rd + 1 < rounds) prefetch(grp + stride);
     phase_sync<SYNC>();
     constexpr int LG = log2k<K>();
     // Interpolate: inverse transform on coset 0, levels 0 .. LG-1.
-    level0_pair<K, 0, true>(r, h0, h1);
-    phase_sync<SYNC>();
-    levels_up<K, 1, 0, true, SYNC>(r);
+    levels_up<K, W, 0, 0, SYNC>(r, q, qm);
     // Evaluate on coset K: forward transform, levels LG-1 .. 0.
-    levels_down<K, LG - 1, K, false, SYNC>(r);
-    level0_pair<K, K, false>(r, h0, h1);
-    phase_sync<SYNC>();
+    levels_down<K, W, LG - 1, K, SYNC>(r, q, qm);
     if (live) {
 #pragma unroll
-      for (int j = 0; j < K / 2; j++) {
+      for (int j = 0; j < S; j++) {
         uint8_t *row;
         if constexpr (PTRS)
-          row = pt.out[2 * j + h1];
+          row = pt.out[(j << W) | q];
         else
-          row = loc.out0 + (uint64_t)(2 * j + h1) * loc.out_rs;
+          row = loc.out0 + (uint64_t)((j << W) | q) * loc.out_rs;
         uint32_t w[8];
 #pragma unroll
         for (int b = 0; b < 8; b++) w[b] = r[j][b];
@@ -462,7 +499,7 @@ __global__ void __launch_bounds__(THREADS, CTAS)
 
 // Selected launch shape (index into kFftVariants); set by rs_set_fft_variant.
 inline int &fft_variant() {
-  static int v = 1;
+  static int v = 0;
   return v;
 }
 
@@ -482,20 +519,32 @@ struct FftShape {
 };
 
 inline const FftShape *find_fft_shape(size_t k, size_t m) {
-  static const FftShape shapes[] = {{2, 2}, {4, 4}, {8, 8}, {16, 16}, {32, 32}};
+  static const FftShape shapes[] = {{2, 2}, {4, 4}, {8, 8}, {16, 16}, {32, 32}, {64, 64}, {128, 128}};
   for (const FftShape &s : shapes)
     if ((size_t)s.k == k && (size_t)s.m == m) return &s;
   return nullptr;
 }
 
-template <int K, bool PTRS, int V>
-inline cudaError_t launch_fft_kv(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
+// Lane-group widths tried per K (lanes per group = 2^W, slots per lane = K >> W).
+constexpr int fft_w_lo(int K) { return K <= 8 ? 1 : K <= 32 ? 1 : K == 64 ? 2 : 3; }
+constexpr int fft_w_hi(int K) { return K <= 8 ? 1 : K <= 32 ? 2 : K == 64 ? 3 : 4; }
+
+// Selected lane-group width per K: 0 = fft_w_lo, 1 = fft_w_hi (rs_set_fft_lanes).
+inline int &fft_lanes_choice(int K) {
+  static int c[8] = {1, 1, 1, 1, 1, 1, 1, 1};
+  int l = 0;
+  while ((1 << l) < K) l++;
+  return c[l & 7];
+}
+
+template <int K, int W, bool PTRS, int V>
+inline cudaError_t launch_fft_kwv(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
   constexpr FftVariant var = kFftVariants[V];
-  uint64_t pairs = a.items ? a.total_groups : (uint64_t)a.n_stripes * a.groups_per_stripe;
-  uint64_t blocks = (pairs * 2 + var.threads - 1) / var.threads;
+  uint64_t groups = a.items ? a.total_groups : (uint64_t)a.n_stripes * a.groups_per_stripe;
+  uint64_t blocks = ((groups << W) + var.threads - 1) / var.threads;
   blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, (uint64_t)sm_count() * var.ctas));
-  const int smem = (K / 2) * FftStage<var.threads>::kSlot;
-  auto kern = fft_kk_kernel<K, PTRS, var.threads, var.ctas, (bool)var.sync>;
+  const int smem = (K >> W) * FftStage<var.threads>::kSlot;
+  auto kern = fft_kk_kernel<K, W, PTRS, var.threads, var.ctas, (bool)var.sync>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -504,17 +553,64 @@ inline cudaError_t launch_fft_kv(const FftArgs &a, const PtrTableT<PTRS> &pt, cu
   return cudaGetLastError();
 }
 
+template <int K, int W, bool PTRS>
+inline cudaError_t launch_fft_kw(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
+  if constexpr (PTRS) {
+    return launch_fft_kwv<K, W, PTRS, 0>(a, pt, st);  // single-stripe calls
+  } else {
+    if (fft_variant() == 1) return launch_fft_kwv<K, W, PTRS, 1>(a, pt, st);
+    return launch_fft_kwv<K, W, PTRS, 0>(a, pt, st);
+  }
+}
+
 template <int K, bool PTRS>
 inline cudaError_t launch_fft_k(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
-  if constexpr (PTRS) return launch_fft_kv<K, PTRS, 1>(a, pt, st);  // single-stripe calls
-  switch (fft_variant()) {
-    case 0: return launch_fft_kv<K, PTRS, 0>(a, pt, st);
-    case 2: return launch_fft_kv<K, PTRS, 2>(a, pt, st);
-    case 3: return launch_fft_kv<K, PTRS, 3>(a, pt, st);
-    case 4: return launch_fft_kv<K, PTRS, 4>(a, pt, st);
-    case 5: return launch_fft_kv<K, PTRS, 5>(a, pt, st);
-    default: return launch_fft_kv<K, PTRS, 1>(a, pt, st);
+  if constexpr (fft_w_lo(K) == fft_w_hi(K)) {
+    return launch_fft_kw<K, fft_w_lo(K), PTRS>(a, pt, st);
+  } else {
+    if (fft_lanes_choice(K)) return launch_fft_kw<K, fft_w_hi(K), PTRS>(a, pt, st);
+    return launch_fft_kw<K, fft_w_lo(K), PTRS>(a, pt, st);
   }
+}
+
+// Per-K launchers, each compiled in its own translation unit (fft_k*.cu) so the large
+// straight-line kernels build in parallel.
+#define RSB_FFT_DECLARE(K)                                                                     \
+  cudaError_t fft_launch_k##K(const FftArgs &a, const PtrTableT<false> &pt, cudaStream_t st); \
+  cudaError_t fft_launch_k##K##p(const FftArgs &a, const PtrTableT<true> &pt, cudaStream_t st);
+#define RSB_FFT_DEFINE(K)                                                                      \
+  cudaError_t fft_launch_k##K(const FftArgs &a, const PtrTableT<false> &pt, cudaStream_t st) { \
+    return launch_fft_k<K, false>(a, pt, st);                                                  \
+  }                                                                                            \
+  cudaError_t fft_launch_k##K##p(const FftArgs &a, const PtrTableT<true> &pt, cudaStream_t st) { \
+    return launch_fft_k<K, true>(a, pt, st);                                                   \
+  }
+RSB_FFT_DECLARE(2)
+RSB_FFT_DECLARE(4)
+RSB_FFT_DECLARE(8)
+RSB_FFT_DECLARE(16)
+RSB_FFT_DECLARE(32)
+RSB_FFT_DECLARE(64)
+RSB_FFT_DECLARE(128)
+
+template <int K, bool PTRS>
+inline cudaError_t fft_launch_extern(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
+#define RSB_FFT_CALL(KK)                        \
+  if constexpr (K == KK) {                      \
+    if constexpr (PTRS)                         \
+      return fft_launch_k##KK##p(a, pt, st);    \
+    else                                        \
+      return fft_launch_k##KK(a, pt, st);       \
+  }
+  RSB_FFT_CALL(2)
+  RSB_FFT_CALL(4)
+  RSB_FFT_CALL(8)
+  RSB_FFT_CALL(16)
+  RSB_FFT_CALL(32)
+  RSB_FFT_CALL(64)
+  RSB_FFT_CALL(128)
+#undef RSB_FFT_CALL
+  return cudaErrorInvalidValue;
 }
 
 template <bool PTRS>
@@ -523,11 +619,13 @@ inline int launch_fft_any(const FftShape &sh, const FftArgs &a, const PtrTableT<
   if (a.items ? a.total_groups == 0 : (a.len == 0 || a.n_stripes == 0)) return RS_OK;
   cudaError_t e;
   switch (sh.k) {
-    case 2: e = launch_fft_k<2, PTRS>(a, pt, st); break;
-    case 4: e = launch_fft_k<4, PTRS>(a, pt, st); break;
-    case 8: e = launch_fft_k<8, PTRS>(a, pt, st); break;
-    case 16: e = launch_fft_k<16, PTRS>(a, pt, st); break;
-    case 32: e = launch_fft_k<32, PTRS>(a, pt, st); break;
+    case 2: e = fft_launch_extern<2, PTRS>(a, pt, st); break;
+    case 4: e = fft_launch_extern<4, PTRS>(a, pt, st); break;
+    case 8: e = fft_launch_extern<8, PTRS>(a, pt, st); break;
+    case 16: e = fft_launch_extern<16, PTRS>(a, pt, st); break;
+    case 32: e = fft_launch_extern<32, PTRS>(a, pt, st); break;
+    case 64: e = fft_launch_extern<64, PTRS>(a, pt, st); break;
+    case 128: e = fft_launch_extern<128, PTRS>(a, pt, st); break;
     default: return RS_ERR_INVALID_ARGUMENT;
   }
   g_launches++;

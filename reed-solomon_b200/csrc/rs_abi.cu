@@ -302,6 +302,14 @@ int rs_set_fft_variant(int variant) {
 
 int rs_fft_variant_count(void) { return kFftVariantCount; }
 
+int rs_set_fft_lanes(size_t k, int wide) {
+  if (!find_fft_shape(k, k) || wide < 0 || wide > 1) return -1;
+  int &c = fft_lanes_choice((int)k);
+  int old = c;
+  c = wide;
+  return old;
+}
+
 int rs_generator_rows(int field, size_t k, size_t m, uint16_t *out, size_t out_len) {
   if (!out || (field != 8 && field != 16)) return RS_ERR_INVALID_ARGUMENT;
   if (k == 0) return RS_TOO_FEW_DATA_SHARDS;
