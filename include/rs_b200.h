@@ -267,14 +267,19 @@ int rs_decode_rows(int field, size_t k, size_t m, const uint8_t *present, uint16
                    size_t out_len, size_t *n_rows);
 /* Number of this library's kernel launches so far in this process. */
 uint64_t rs_kernel_launch_count(void);
-/* Tuning hook (autotuner): launch shape of the bitsliced FFT kernel for batched calls,
- * 0..rs_fft_variant_count()-1. Returns the previous value, or -1 if out of range. */
-int rs_set_fft_variant(int variant);
+/* Tuning hook (autotuner): launch shape of the (k,k) bitsliced FFT kernel for batched
+ * calls, 0..rs_fft_variant_count()-1 (CTAs per SM). Returns the previous value, or -1
+ * when out of range or (k,k) has no FFT kernel. */
+int rs_set_fft_variant(size_t k, int variant);
 int rs_fft_variant_count(void);
 /* Tuning hook: lane-group width of the (k,k) FFT kernel, 0 = narrow, 1 = wide (more
  * lanes per 32-column group, fewer registers per lane). Returns the previous value,
  * or -1 when (k,k) has no FFT kernel. */
 int rs_set_fft_lanes(size_t k, int wide);
+/* Tuning hook: tile shape of the matrix kernel for batched and single calls
+ * (parity rows per thread x output rows per CTA), 0..rs_matrix_variant_count()-1. */
+int rs_set_matrix_variant(int variant);
+int rs_matrix_variant_count(void);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -24,9 +24,11 @@ SIGNATURES = {
     "rs_abi_version": (ctypes.c_uint32, []),
     "rs_device_check": (_int, []),
     "rs_kernel_launch_count": (ctypes.c_uint64, []),
-    "rs_set_fft_variant": (_int, [_int]),
+    "rs_set_fft_variant": (_int, [_sz, _int]),
     "rs_fft_variant_count": (_int, []),
     "rs_set_fft_lanes": (_int, [_sz, _int]),
+    "rs_set_matrix_variant": (_int, [_int]),
+    "rs_matrix_variant_count": (_int, []),
     "rs_generator_rows": (_int, [_int, _sz, _sz, _u16p, _sz]),
     "rs_decode_rows": (_int, [_int, _sz, _sz, _u8p, _u16p, _sz, _szp]),
     "rs8_new": (_int, [_sz, _sz, _pp]),

@@ -498,9 +498,13 @@ __global__ void __launch_bounds__(THREADS, CTAS)
 }
 
 // Selected launch shape (index into kFftVariants); set by rs_set_fft_variant.
-inline int &fft_variant() {
-  static int v = 0;
-  return v;
+// Per-K launch shape (index into kFftVariants), defaults from a sweep on B200:
+// K = 16 and 64 prefer 4 CTAs/SM, the others 3.
+inline int &fft_variant_for(int K) {
+  static int v[8] = {0, 0, 0, 0, 1, 0, 1, 0};
+  int l = 0;
+  while ((1 << l) < K) l++;
+  return v[l & 7];
 }
 
 inline int sm_count() {
@@ -531,7 +535,7 @@ constexpr int fft_w_hi(int K) { return K <= 8 ? 1 : K <= 32 ? 2 : K == 64 ? 3 : 
 
 // Selected lane-group width per K: 0 = fft_w_lo, 1 = fft_w_hi (rs_set_fft_lanes).
 inline int &fft_lanes_choice(int K) {
-  static int c[8] = {1, 1, 1, 1, 1, 1, 1, 1};
+  static int c[8] = {0, 0, 0, 0, 0, 0, 1, 0};  // wide groups only for K = 64
   int l = 0;
   while ((1 << l) < K) l++;
   return c[l & 7];
@@ -558,7 +562,7 @@ inline cudaError_t launch_fft_kw(const FftArgs &a, const PtrTableT<PTRS> &pt, cu
   if constexpr (PTRS) {
     return launch_fft_kwv<K, W, PTRS, 0>(a, pt, st);  // single-stripe calls
   } else {
-    if (fft_variant() == 1) return launch_fft_kwv<K, W, PTRS, 1>(a, pt, st);
+    if (fft_variant_for(K) == 1) return launch_fft_kwv<K, W, PTRS, 1>(a, pt, st);
     return launch_fft_kwv<K, W, PTRS, 0>(a, pt, st);
   }
 }

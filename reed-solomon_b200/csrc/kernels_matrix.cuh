@@ -22,7 +22,18 @@ namespace rsb {
 constexpr int kThreads = 256;
 constexpr int kBytesPerThread = 16;
 constexpr int kTileBytes = kThreads * kBytesPerThread;  // 4 KiB of columns per CTA
-constexpr uint32_t kRowChunk = 32;    // GF(2^8) output rows per CTA (grid.z)
+constexpr uint32_t kRowChunk = 32;    // GF(2^8) output rows per CTA (grid.z), default tile
+// Tile shapes of the matrix kernel: parity rows accumulated per thread (registers) and
+// output rows per CTA (grid.z chunk). Chosen per call by the autotuner.
+struct MatrixVariant {
+  int out_tile, row_chunk;
+};
+constexpr MatrixVariant kMatrixVariants[] = {{8, 32}, {4, 16}, {8, 64}, {16, 64}};
+constexpr int kMatrixVariantCount = sizeof(kMatrixVariants) / sizeof(kMatrixVariants[0]);
+inline int &matrix_variant() {
+  static int v = 0;
+  return v;
+}
 constexpr uint32_t kRowChunk16 = 64;  // tower output rows per CTA (grid.z)
 
 // Addressing of one launch: either pointer tables passed by value as a kernel
@@ -140,7 +151,7 @@ __device__ __forceinline__ uint8_t *out_row(const ApplyArgs &a, const PtrTableT<
 
 // grid.x: column tiles of kTileBytes; grid.y: stripes (looped when more than grid.y).
 // Dynamic shared memory: 8 KiB constant table + rows*k coefficient bytes.
-template <int OUT_TILE, bool PTRS, bool VERIFY>
+template <int OUT_TILE, int ROW_CHUNK, bool PTRS, bool VERIFY>
 __global__ void __launch_bounds__(kThreads)
     gf8_matrix_kernel(const ApplyArgs a, const __grid_constant__ PtrTableT<PTRS> pt) {
   extern __shared__ __align__(16) uint32_t smem[];
@@ -156,9 +167,9 @@ __global__ void __launch_bounds__(kThreads)
     __syncthreads();
     if (col < a.len) {
       const uint64_t remain = a.len - col;
-      // grid.z splits the output rows into chunks of kRowChunk.
-      const uint32_t g_end = min(rows, (blockIdx.z + 1) * kRowChunk);
-      for (uint32_t g = blockIdx.z * kRowChunk; g < g_end; g += OUT_TILE) {
+      // grid.z splits the output rows into chunks of ROW_CHUNK.
+      const uint32_t g_end = min(rows, (blockIdx.z + 1) * ROW_CHUNK);
+      for (uint32_t g = blockIdx.z * ROW_CHUNK; g < g_end; g += OUT_TILE) {
         const uint32_t live = g_end - g;
         uint32_t acc[OUT_TILE][4];
 #pragma unroll

@@ -74,13 +74,14 @@ const Gf16Tables &gf16() {
 
 static size_t g8_smem(uint32_t rows, uint32_t k) { return 8192 + (size_t)rows * k; }
 
-template <int OT, bool PTRS, bool VERIFY>
+template <int V, bool PTRS, bool VERIFY>
 static int launch_gf8_t(const ApplyArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
-  auto kern = gf8_matrix_kernel<OT, PTRS, VERIFY>;
+  constexpr MatrixVariant mv = kMatrixVariants[V];
+  auto kern = gf8_matrix_kernel<mv.out_tile, mv.row_chunk, PTRS, VERIFY>;
   size_t smem = g8_smem(a.rows, a.k);
   if (smem > 48 * 1024) RSB_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   uint64_t tiles = (a.len + kTileBytes - 1) / kTileBytes;
-  dim3 grid((unsigned)tiles, std::min<uint32_t>(a.n_stripes, 65535), (a.rows + kRowChunk - 1) / kRowChunk);
+  dim3 grid((unsigned)tiles, std::min<uint32_t>(a.n_stripes, 65535), (a.rows + mv.row_chunk - 1) / mv.row_chunk);
   kern<<<grid, kThreads, smem, st>>>(a, pt);
   g_launches++;
   RSB_CU(cudaGetLastError());
@@ -93,10 +94,16 @@ int launch_gf8(const ApplyArgs &a, const PtrTable *pt, bool verify, cudaStream_t
     PtrTableT<true> t;
     memcpy(t.in, pt->in, sizeof(t.in));
     memcpy(t.out, pt->out, sizeof(t.out));
-    return verify ? launch_gf8_t<8, true, true>(a, t, st) : launch_gf8_t<8, true, false>(a, t, st);
+    return verify ? launch_gf8_t<0, true, true>(a, t, st) : launch_gf8_t<0, true, false>(a, t, st);
   }
   PtrTableT<false> t{};
-  return verify ? launch_gf8_t<8, false, true>(a, t, st) : launch_gf8_t<8, false, false>(a, t, st);
+  if (verify) return launch_gf8_t<0, false, true>(a, t, st);
+  switch (matrix_variant()) {
+    case 1: return launch_gf8_t<1, false, false>(a, t, st);
+    case 2: return launch_gf8_t<2, false, false>(a, t, st);
+    case 3: return launch_gf8_t<3, false, false>(a, t, st);
+    default: return launch_gf8_t<0, false, false>(a, t, st);
+  }
 }
 
 // ------------------------------------------------------------------------------
@@ -293,14 +300,24 @@ int rs_device_check(void) { return ensure_device(nullptr); }
 
 uint64_t rs_kernel_launch_count(void) { return g_launches.load(); }
 
-int rs_set_fft_variant(int variant) {
-  if (variant < 0 || variant >= kFftVariantCount) return -1;
-  int old = fft_variant();
-  fft_variant() = variant;
+int rs_set_fft_variant(size_t k, int variant) {
+  if (!find_fft_shape(k, k) || variant < 0 || variant >= kFftVariantCount) return -1;
+  int &v = fft_variant_for((int)k);
+  int old = v;
+  v = variant;
   return old;
 }
 
 int rs_fft_variant_count(void) { return kFftVariantCount; }
+
+int rs_set_matrix_variant(int variant) {
+  if (variant < 0 || variant >= kMatrixVariantCount) return -1;
+  int old = matrix_variant();
+  matrix_variant() = variant;
+  return old;
+}
+
+int rs_matrix_variant_count(void) { return kMatrixVariantCount; }
 
 int rs_set_fft_lanes(size_t k, int wide) {
   if (!find_fft_shape(k, k) || wide < 0 || wide > 1) return -1;
