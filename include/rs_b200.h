@@ -251,6 +251,26 @@ int gf8_mul_slice(uint8_t *out, size_t out_len, const uint8_t *in, size_t in_len
 int gf8_mul_slice_dev(uint8_t *d_out, const uint8_t *d_in, size_t n, uint8_t c, int xor_into,
                       void *stream);
 
+/* ========================== learned cost model (MLP) ==========================
+ * No counterpart in the reference. An FP32 MLP (n_in -> hidden x3 ReLU -> n_out)
+ * trained and evaluated on the GPU by this library's kernels; the tuner maps a
+ * workload's features to one predicted log-time per candidate launch configuration.
+ * Device arrays are row-major float: x [batch x n_in], y and mask [batch x n_out]. */
+typedef struct rs_mlp rs_mlp_t;
+int rs_mlp_create(int n_in, int hidden, int n_out, uint64_t seed, rs_mlp_t **out);
+void rs_mlp_free(rs_mlp_t *mlp);
+size_t rs_mlp_param_count(const rs_mlp_t *mlp);
+int rs_mlp_get_params(const rs_mlp_t *mlp, float *out, size_t n);
+int rs_mlp_set_params(rs_mlp_t *mlp, const float *in, size_t n);
+int rs_mlp_predict(rs_mlp_t *mlp, const float *d_x, int batch, float *d_out);
+/* Gradients of the masked mean squared error (sum over mask / mask_count) for every
+ * parameter, in parameter order, into host memory; no update. */
+int rs_mlp_gradients(rs_mlp_t *mlp, const float *d_x, const float *d_y, const float *d_mask, int batch,
+                     float mask_count, float *grads_out, size_t n, float *loss);
+/* One Adam step on the batch; *loss (optional) receives the loss before the step. */
+int rs_mlp_train_step(rs_mlp_t *mlp, const float *d_x, const float *d_y, const float *d_mask, int batch,
+                      float mask_count, float lr, float *loss);
+
 /* ============================ device / diagnostics ============================ */
 
 /* 0 when a CUDA device is usable, RS_ERR_NO_DEVICE otherwise. */

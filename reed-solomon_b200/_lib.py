@@ -84,6 +84,16 @@ SIGNATURES = {
     "rs16_encode_dev": (_int, [_vp, _pp, _sz, _sz, _vp]),
     "rs16_encode_batch_dev": (_int, [_vp, _vp, _sz, _vp, _sz, _sz, _sz, _vp]),
     "rs16_reconstruct_dev": (_int, [_vp, _pp, _szp, _u8p, _sz, _int, _vp]),
+    "rs_mlp_create": (_int, [_int, _int, _int, ctypes.c_uint64, _pp]),
+    "rs_mlp_free": (None, [_vp]),
+    "rs_mlp_param_count": (_sz, [_vp]),
+    "rs_mlp_get_params": (_int, [_vp, _vp, _sz]),
+    "rs_mlp_set_params": (_int, [_vp, _vp, _sz]),
+    "rs_mlp_predict": (_int, [_vp, _vp, _int, _vp]),
+    "rs_mlp_gradients": (_int, [_vp, _vp, _vp, _vp, _int, ctypes.c_float, _vp, _sz,
+                                ctypes.POINTER(ctypes.c_float)]),
+    "rs_mlp_train_step": (_int, [_vp, _vp, _vp, _vp, _int, ctypes.c_float, ctypes.c_float,
+                                 ctypes.POINTER(ctypes.c_float)]),
     "gf8_mul_slice": (_int, [_vp, _sz, _vp, _sz, ctypes.c_uint8, _int]),
     "gf8_mul_slice_dev": (_int, [_vp, _vp, _sz, ctypes.c_uint8, _int, _vp]),
 }

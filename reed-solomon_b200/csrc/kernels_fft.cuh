@@ -369,12 +369,19 @@ __device__ __forceinline__ FftLoc fft_locate(const FftArgs &a, uint64_t pair) {
   }
   const uint64_t total = (uint64_t)a.n_stripes * a.groups_per_stripe;
   if (pair >= total) return l;
-  const uint32_t s = (uint32_t)(pair / a.groups_per_stripe);
+  uint32_t s, g;
+  if (total <= 0xffffffffull) {  // 32-bit division: the common case, far cheaper
+    s = (uint32_t)pair / a.groups_per_stripe;
+    g = (uint32_t)pair - s * a.groups_per_stripe;
+  } else {
+    s = (uint32_t)(pair / a.groups_per_stripe);
+    g = (uint32_t)(pair - (uint64_t)s * a.groups_per_stripe);
+  }
   l.in0 = a.in_base + s * a.in_stripe_stride;
   l.out0 = a.out_base + s * a.out_stripe_stride;
   l.in_rs = a.in_row_stride;
   l.out_rs = a.out_row_stride;
-  l.col = (pair % a.groups_per_stripe) * 32;
+  l.col = (uint64_t)g * 32;
   l.remain = a.len - l.col;
   return l;
 }
@@ -461,15 +468,25 @@ __global__ void __launch_bounds__(THREADS, CTAS)
     const bool live = loc.remain != 0;
     const uint64_t col = loc.col, remain = loc.remain;
     cp_async_wait_all();
+    // Bytes -> bit planes in place, one rolled loop: the transpose code appears once
+    // instead of once per slot, keeping the loop body small for the instruction cache.
+#pragma unroll 1
+    for (int j = 0; j < S; j++) {
+      uint4 *p0 = reinterpret_cast<uint4 *>(mine + j * St::kSlot);
+      uint4 *p1 = reinterpret_cast<uint4 *>(mine + j * St::kSlot + St::kHalf);
+      uint4 lo = *p0, hi = *p1;
+      uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+      bit_transpose(w);
+      *p0 = make_uint4(w[0], w[1], w[2], w[3]);
+      *p1 = make_uint4(w[4], w[5], w[6], w[7]);
+    }
     Reg r[S];
 #pragma unroll
     for (int j = 0; j < S; j++) {
       uint4 lo = *reinterpret_cast<const uint4 *>(mine + j * St::kSlot);
       uint4 hi = *reinterpret_cast<const uint4 *>(mine + j * St::kSlot + St::kHalf);
-      uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
-      bit_transpose(w);
-#pragma unroll
-      for (int b = 0; b < 8; b++) r[j][b] = w[b];
+      r[j][0] = lo.x, r[j][1] = lo.y, r[j][2] = lo.z, r[j][3] = lo.w;
+      r[j][4] = hi.x, r[j][5] = hi.y, r[j][6] = hi.z, r[j][7] = hi.w;
     }
     if (rd + 1 < rounds) prefetch(grp + stride);
     phase_sync<SYNC>();

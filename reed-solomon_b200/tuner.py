@@ -1,0 +1,261 @@
+"""Autotuner and learned cost model for route and tile choice.
+
+The autotuner times every candidate launch configuration of a workload on the GPU
+(exhaustive tuning); those timings train the cost model, an FP32 MLP trained and run by
+this library's CUDA kernels (rs_mlp_*), which then predicts the best configuration for
+unseen workloads without timing them. Configurations only choose kernels and launch
+shapes, never arithmetic, so every choice yields the same bytes.
+
+Candidates (GF(2^8)):
+  matrix route, tile variant 0..3 (parity rows per thread x output rows per CTA)
+  FFT route ((K,K) shapes), lane-group width narrow/wide x CTAs per SM 3/4
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from .coder import ReedSolomon, _check
+
+CONFIGS = [("matrix", 0), ("matrix", 1), ("matrix", 2), ("matrix", 3),
+           ("fft", (0, 0)), ("fft", (0, 1)), ("fft", (1, 0)), ("fft", (1, 1))]
+N_FEATURES = 5
+FFT_K = (2, 4, 8, 16, 32, 64, 128)
+
+
+class Workload:
+    """k data + m parity shards of `shard_bytes`, `erasures` rebuilt per stripe
+    (0 = encode), `batch` stripes per launch."""
+
+    def __init__(self, k, m, shard_bytes, erasures=0, batch=1):
+        self.k, self.m, self.shard_bytes, self.erasures, self.batch = k, m, shard_bytes, erasures, batch
+
+    def features(self):
+        return [math.log2(self.k) / 8.0, math.log2(self.m) / 8.0, math.log2(self.shard_bytes) / 20.0,
+                self.erasures / max(self.m, 1), math.log2(self.batch) / 8.0]
+
+    def bytes(self):
+        return self.batch * self.shard_bytes * (self.k + (self.erasures or self.m))
+
+    def __repr__(self):
+        return "Workload(k=%d, m=%d, bytes=%d, erasures=%d, batch=%d)" % (
+            self.k, self.m, self.shard_bytes, self.erasures, self.batch)
+
+
+def applicable(w, cfg):
+    route, _ = cfg
+    if route == "fft":
+        return w.erasures == 0 and w.k == w.m and w.k in FFT_K and w.shard_bytes >= 64
+    return True
+
+
+def apply_config(codec, w, cfg):
+    """Set the library's tuning hooks for `cfg`."""
+    L = _lib.load()
+    route, v = cfg
+    if route == "matrix":
+        codec.set_route("matrix")
+        L.rs_set_matrix_variant(v)
+    else:
+        codec.set_route("fft")
+        L.rs_set_fft_lanes(w.k, v[0])
+        L.rs_set_fft_variant(w.k, v[1])
+
+
+class Bench:
+    """Device buffers and a timing loop for one workload."""
+
+    def __init__(self, w, seed=0):
+        import torch
+
+        self.w = w
+        self.codec = ReedSolomon(w.k, w.m)
+        g = torch.Generator(device="cuda").manual_seed(seed)
+        n = w.k + w.m
+        self.rows = torch.randint(0, 256, (w.batch, n, w.shard_bytes), dtype=torch.uint8, device="cuda",
+                                  generator=g)
+        self.present = None
+        if w.erasures:
+            rng = np.random.default_rng(seed)
+            self.present = np.ones((w.batch, n), np.uint8)
+            for s in range(w.batch):
+                self.present[s, rng.choice(n, size=w.erasures, replace=False)] = 0
+
+    def run(self):
+        w = self.w
+        if w.erasures:
+            self.codec.reconstruct_batch_dev(self.rows, w.batch, w.shard_bytes, self.present)
+        else:
+            stride = (w.k + w.m) * w.shard_bytes
+            parity = self.rows[:, w.k:]
+            self.codec.encode_batch_dev(self.rows, parity, w.shard_bytes, w.batch, data_stride=stride,
+                                        parity_stride=stride)
+
+    def time(self, cfg, reps=3):
+        import torch
+
+        apply_config(self.codec, self.w, cfg)
+        self.run()
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            self.run()
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
+
+def reset_defaults():
+    L = _lib.load()
+    L.rs_set_matrix_variant(0)
+    for k, (wide, var) in DEFAULT_FFT.items():
+        L.rs_set_fft_lanes(k, wide)
+        L.rs_set_fft_variant(k, var)
+
+
+def exhaustive(w, reps=3, seed=0):
+    """Time every applicable configuration: (times in ms per config, NaN if n/a)."""
+    b = Bench(w, seed)
+    t = np.full(len(CONFIGS), np.nan)
+    for i, cfg in enumerate(CONFIGS):
+        if applicable(w, cfg):
+            t[i] = b.time(cfg, reps)
+    reset_defaults()
+    return t
+
+
+def sample_workloads(n, seed, max_bytes=96 << 20):
+    """GF(2^8) workloads spread like the serving mix: k log-uniform, shard bytes
+    log-uniform 512 B .. 1 MiB, a quarter reconstruct; (K,K) power-of-two shapes
+    over-sampled so the FFT candidates are exercised."""
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < n:
+        if rng.random() < 0.4:
+            k = int(rng.choice([16, 32, 64, 128]))
+            m = k
+        else:
+            k = int(math.exp(rng.uniform(math.log(4), math.log(200))))
+            m = int(rng.integers(2, min(3 * k, 256 - k) + 1)) if 256 - k >= 2 else 1
+            if k + m > 256 or m < 1:
+                continue
+        shard = int(math.exp(rng.uniform(math.log(512), math.log(1 << 20))))
+        erasures = int(rng.integers(1, m + 1)) if rng.random() < 0.25 else 0
+        batch = int(2 ** rng.integers(0, 7))
+        w = Workload(k, m, shard, erasures, batch)
+        while w.bytes() > max_bytes and w.batch > 1:
+            w.batch //= 2
+        if w.bytes() > max_bytes:
+            continue
+        out.append(w)
+    return out
+
+
+def collect(workloads, reps=3):
+    X = np.array([w.features() for w in workloads], np.float32)
+    T = np.stack([exhaustive(w, reps, seed=i) for i, w in enumerate(workloads)])
+    return X, T
+
+
+class CostModel:
+    """FP32 MLP on the GPU (rs_mlp_*): features -> log(ms) per configuration."""
+
+    def __init__(self, hidden=64, seed=1):
+        self._L = _lib.load()
+        h = ctypes.c_void_p()
+        _check(self._L.rs_mlp_create(N_FEATURES, hidden, len(CONFIGS), seed, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._L.rs_mlp_free(h)
+
+    def n_params(self):
+        return self._L.rs_mlp_param_count(self._h)
+
+    def params(self):
+        out = np.zeros(self.n_params(), np.float32)
+        _check(self._L.rs_mlp_get_params(self._h, out.ctypes.data, out.size))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        _check(self._L.rs_mlp_set_params(self._h, p.ctypes.data, p.size))
+
+    @staticmethod
+    def _targets(T):
+        mask = np.isfinite(T).astype(np.float32)
+        Y = np.where(mask > 0, np.log(np.where(mask > 0, T, 1.0)), 0.0).astype(np.float32)
+        return Y, mask
+
+    def gradients(self, X, Y, mask):
+        import torch
+
+        x, y, mk = (torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda() for a in (X, Y, mask))
+        g = np.zeros(self.n_params(), np.float32)
+        loss = ctypes.c_float()
+        _check(self._L.rs_mlp_gradients(self._h, x.data_ptr(), y.data_ptr(), mk.data_ptr(), x.shape[0],
+                                        float(mask.sum()), g.ctypes.data, g.size, ctypes.byref(loss)))
+        return g, loss.value
+
+    def fit(self, X, T, epochs=400, lr=3e-3, batch=512, seed=0):
+        import torch
+
+        Y, mask = self._targets(T)
+        x = torch.from_numpy(np.ascontiguousarray(X, np.float32)).cuda()
+        y = torch.from_numpy(Y).cuda()
+        mk = torch.from_numpy(mask).cuda()
+        rng = np.random.default_rng(seed)
+        n = x.shape[0]
+        loss = ctypes.c_float()
+        history = []
+        for ep in range(epochs):
+            perm = torch.from_numpy(rng.permutation(n)).cuda()
+            for s in range(0, n, batch):
+                idx = perm[s:s + batch]
+                xb, yb, mb = x[idx].contiguous(), y[idx].contiguous(), mk[idx].contiguous()
+                _check(self._L.rs_mlp_train_step(self._h, xb.data_ptr(), yb.data_ptr(), mb.data_ptr(), xb.shape[0],
+                                                 float(mb.sum().item()), lr, ctypes.byref(loss)))
+            history.append(loss.value)
+        return history
+
+    def predict(self, X):
+        import torch
+
+        x = torch.from_numpy(np.ascontiguousarray(X, np.float32)).cuda()
+        out = torch.empty((x.shape[0], len(CONFIGS)), dtype=torch.float32, device="cuda")
+        _check(self._L.rs_mlp_predict(self._h, x.data_ptr(), x.shape[0], out.data_ptr()))
+        return out.cpu().numpy()
+
+    def choose(self, X, T):
+        """Index of the predicted-fastest applicable configuration per row (T gives
+        applicability: NaN = not applicable)."""
+        P = self.predict(X)
+        P = np.where(np.isfinite(T), P, np.inf)
+        return P.argmin(axis=1)
+
+
+DEFAULT_FFT = {2: (0, 0), 4: (0, 0), 8: (0, 0), 16: (0, 1), 32: (0, 0), 64: (1, 1), 128: (0, 0)}
+
+
+def default_choice(workloads, T):
+    """The method without the model: the library's default route and tile (the FFT
+    kernel with its per-K default launch shape where the shape has one, else matrix
+    tile 0)."""
+    out = np.zeros(len(workloads), np.int64)
+    for i, w in enumerate(workloads):
+        if applicable(w, ("fft", (0, 0))) and np.isfinite(T[i, 4]):
+            out[i] = CONFIGS.index(("fft", DEFAULT_FFT[w.k]))
+    return out
+
+
+def regret(T, choice):
+    """Mean of time(chosen) / time(best) - 1 over workloads."""
+    best = np.nanmin(T, axis=1)
+    chosen = T[np.arange(len(T)), choice]
+    return float(np.mean(chosen / best - 1.0))
