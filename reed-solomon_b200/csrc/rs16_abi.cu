@@ -10,6 +10,7 @@
 
 #include "runtime.hpp"
 #include "gf_host.hpp"
+#include "kernels_lagrange.cuh"
 #include "kernels_matrix.cuh"
 
 namespace rsb {
@@ -24,7 +25,6 @@ static inline uint32_t split16(uint16_t c) {
 struct Gen16 {
   int device = 0;
   size_t k = 0, m = 0;
-  std::vector<uint16_t> rows;  // m x k
   uint32_t *d_split = nullptr;
   ~Gen16() {
     if (d_split) {
@@ -34,12 +34,40 @@ struct Gen16 {
   }
 };
 
-static int upload_split(const std::vector<uint16_t> &rows, uint32_t **out) {
-  std::vector<uint32_t> split(rows.size());
-  for (size_t t = 0; t < rows.size(); t++) split[t] = split16(rows[t]);
-  RSB_CU(cudaMalloc(out, std::max<size_t>(split.size(), 1) * 4));
-  RSB_CU(cudaMemcpy(*out, split.data(), split.size() * 4, cudaMemcpyHostToDevice));
-  return RS_OK;
+// Lagrange rows from `nodes` to `targets`, built on the device as split constants
+// (kernels_lagrange.cuh). *out is a fresh device allocation of targets x nodes u32.
+static int lagrange16_device(const std::vector<uint16_t> &nodes, const std::vector<uint16_t> &targets,
+                             uint32_t **out) {
+  const uint32_t k = (uint32_t)nodes.size(), nt = (uint32_t)targets.size();
+  const size_t entries = std::max<size_t>((size_t)k * nt, 1);
+  RSB_CU(cudaMalloc(out, entries * 4));
+  if (!k || !nt) return RS_OK;
+  // scratch: nodes | targets | w | ell | hit
+  size_t off_t = (k * 2 + 15) & ~size_t(15), off_w = off_t + ((nt * 2 + 15) & ~size_t(15));
+  size_t off_e = off_w + ((k * 2 + 15) & ~size_t(15)), off_h = off_e + ((nt * 2 + 15) & ~size_t(15));
+  size_t bytes = off_h + nt * 4;
+  uint8_t *s = nullptr;
+  RSB_CU(cudaMalloc(&s, bytes));
+  int st = RS_OK;
+  do {
+    uint16_t *d_nodes = reinterpret_cast<uint16_t *>(s), *d_t = reinterpret_cast<uint16_t *>(s + off_t);
+    uint16_t *d_w = reinterpret_cast<uint16_t *>(s + off_w), *d_ell = reinterpret_cast<uint16_t *>(s + off_e);
+    uint32_t *d_hit = reinterpret_cast<uint32_t *>(s + off_h);
+    if (cudaMemcpy(d_nodes, nodes.data(), k * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_t, targets.data(), nt * 2, cudaMemcpyHostToDevice) != cudaSuccess) {
+      st = RS_ERR_CUDA;
+      break;
+    }
+    lagrange16_weights<<<(k + 255) / 256, 256>>>(d_nodes, k, d_w);
+    lagrange16_ell<<<(nt + 255) / 256, 256>>>(d_nodes, k, d_t, nt, d_ell, d_hit);
+    uint64_t n = (uint64_t)k * nt;
+    lagrange16_rows<<<(unsigned)((n + 255) / 256), 256>>>(d_nodes, k, d_t, nt, d_w, d_ell, d_hit, *out, nullptr);
+    g_launches += 3;
+    if (cudaDeviceSynchronize() != cudaSuccess) st = RS_ERR_CUDA;
+  } while (0);
+  if (st) set_cuda_error(cudaGetLastError(), "lagrange16_device");
+  cudaFree(s);
+  return st;
 }
 
 static int launch_gf16(const Apply16Args &a, bool verify, cudaStream_t st) {
@@ -81,7 +109,7 @@ struct rs16_decoder {
 namespace rsb {
 
 // Plan of one presence pattern: closed-form Lagrange rows from the survivors to each
-// missing shard (data ascending, then parity ascending), built on the host.
+// missing shard (data ascending, then parity ascending), built on the device.
 static int plan16_for(const Gen16 &g, PlanCache &cache, const Presence &pres,
                       std::shared_ptr<const Plan> &out) {
   out = cache.find(pres);
@@ -91,15 +119,14 @@ static int plan16_for(const Gen16 &g, PlanCache &cache, const Presence &pres,
   plan->device = g.device;
   split_pattern(pres, g.k, g.k + g.m, plan->survivors, plan->missing_data, plan->missing_parity);
   if (plan->survivors.size() < g.k) return RS_TOO_FEW_SHARDS_PRESENT;
-  std::vector<size_t> nodes(plan->survivors.begin(), plan->survivors.end());
-  std::vector<size_t> targets(plan->missing_data.begin(), plan->missing_data.end());
+  std::vector<uint16_t> nodes(plan->survivors.begin(), plan->survivors.end());
+  std::vector<uint16_t> targets(plan->missing_data.begin(), plan->missing_data.end());
   targets.insert(targets.end(), plan->missing_parity.begin(), plan->missing_parity.end());
-  std::vector<uint16_t> rows;
-  lagrange_rows<F16>(nodes, targets, rows);
   RSB_CU(cudaSetDevice(g.device));
   uint32_t *d = nullptr;
-  RSB_TRY(upload_split(rows, &d));
+  int st = lagrange16_device(nodes, targets, &d);
   plan->d_rows = d;
+  if (st) return st;
   out = cache.insert(pres, plan);
   return RS_OK;
 }
@@ -202,10 +229,13 @@ int rs16_new(size_t k, size_t m, rs16_t **out) {
   gen->device = dev;
   gen->k = k;
   gen->m = m;
-  parity_rows<F16>(k, m, gen->rows);
+  std::vector<uint16_t> nodes(k), targets(m);
+  for (size_t i = 0; i < k; i++) nodes[i] = (uint16_t)i;
+  for (size_t j = 0; j < m; j++) targets[j] = (uint16_t)(k + j);
   uint32_t *d = nullptr;
-  RSB_TRY(upload_split(gen->rows, &d));
+  int st0 = lagrange16_device(nodes, targets, &d);
   gen->d_split = d;
+  if (st0) return st0;
   auto c = new (std::nothrow) rs16_codec();
   if (!c) return RS_ERR_ALLOC;
   c->gen = gen;
@@ -244,10 +274,18 @@ int rs16_equal(const rs16_t *a, const rs16_t *b) {
   return a->gen->k == b->gen->k && a->gen->m == b->gen->m;
 }
 
+// The generator rows as the device kernels apply them: read back the split constants
+// and join them (c_lo = k0, c_hi = k1 ^ k0).
 int rs16_parity_matrix(const rs16_t *c, uint16_t *out, size_t out_len) {
   if (!c || !out) return RS_ERR_INVALID_ARGUMENT;
-  if (out_len != c->gen->rows.size()) return RS_INCORRECT_SHARD_SIZE;
-  memcpy(out, c->gen->rows.data(), out_len * 2);
+  if (out_len != c->gen->k * c->gen->m) return RS_INCORRECT_SHARD_SIZE;
+  std::vector<uint32_t> split(out_len);
+  RSB_CU(cudaSetDevice(c->gen->device));
+  RSB_CU(cudaMemcpy(split.data(), c->gen->d_split, out_len * 4, cudaMemcpyDeviceToHost));
+  for (size_t t = 0; t < out_len; t++) {
+    uint8_t lo = split[t] & 0xff, hi = (uint8_t)((split[t] >> 8) ^ lo);
+    out[t] = (uint16_t)((hi << 8) | lo);
+  }
   return RS_OK;
 }
 
