@@ -55,7 +55,8 @@ enum rs_status {
   RS_ERR_INVALID_ARGUMENT = 102, /* null handle/pointer or unsupported option */
   RS_ERR_NO_DEVICE = 103,     /* no usable CUDA device */
   RS_ERR_TIMEOUT = 104,       /* a bounded device wait gave up */
-  RS_ERR_LENGTH_MISMATCH = 105 /* gf8_mul_slice lengths differ (the reference panics) */
+  RS_ERR_LENGTH_MISMATCH = 105, /* gf8_mul_slice lengths differ (the reference panics) */
+  RS_ERR_TOO_LARGE = 106       /* the request needs more than a fixed working area holds */
 };
 
 /* Message text for a status (src/errors.rs:24-41 for 1..14). Never NULL. */
@@ -160,6 +161,29 @@ int rs8_reconstruct_dev(rs8_t *codec, uint8_t *const *d_shards, const size_t *le
 int rs8_reconstruct_batch_dev(rs8_t *codec, uint8_t *d_rows, size_t stripe_stride,
                               size_t n_stripes, size_t row_len, const uint8_t *present,
                               int data_only, int *statuses, void *stream);
+
+/* Batched reconstruct that allocates nothing. No counterpart in the reference.
+ * For callers that cannot allocate device memory while they run: a latency-critical
+ * path that must not stall on the allocator, a process whose memory budget was fixed
+ * at start-up, or a host whose device allocator belongs to another framework. Same
+ * arguments, checks and results as rs8_reconstruct_batch_dev, but all working memory
+ * (survivor and target lists, decode rows, plan statuses) lives in one 8 MiB device
+ * array inside this library, which every GPU that loads the library holds until the
+ * process exits, and the host side stages through one fixed buffer: no cudaMalloc,
+ * cudaFree or other allocating call is made. A call needing more than 8 MiB of working
+ * memory (see rs8_reconstruct_batch_noalloc_limit) returns RS_ERR_TOO_LARGE; split the
+ * batch. The first call on each device looks up the array's device address; make that
+ * first call before capturing any stream on that device. Nothing in the array has to
+ * start at zero: each call writes every entry it reads before reading it. Every call
+ * shares the one array and it keeps the last call's contents: calls whose GPU work
+ * overlaps (other streams, or other host threads) race on it, so run them one after
+ * another. */
+int rs8_reconstruct_batch_noalloc(rs8_t *codec, uint8_t *d_rows, size_t stripe_stride,
+                                  size_t n_stripes, size_t row_len, const uint8_t *present,
+                                  int data_only, int *statuses, void *stream);
+/* Bytes of that fixed working area a call of this shape and stripe count needs. */
+size_t rs8_reconstruct_batch_noalloc_limit(size_t data_shards, size_t parity_shards,
+                                           size_t n_stripes);
 
 /* ---- mixed batches: stripes of any GF(2^8) shapes, lengths and erasure patterns ----
  * No counterpart in the reference (it codes one stripe per call on one core). A batch

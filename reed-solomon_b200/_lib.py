@@ -59,6 +59,8 @@ SIGNATURES = {
     "rs8_verify_dev": (_int, [_vp, _pp, _sz, _sz, _intp, _vp]),
     "rs8_reconstruct_dev": (_int, [_vp, _pp, _szp, _u8p, _sz, _int, _vp]),
     "rs8_reconstruct_batch_dev": (_int, [_vp, _vp, _sz, _sz, _sz, _u8p, _int, _intp, _vp]),
+    "rs8_reconstruct_batch_noalloc": (_int, [_vp, _vp, _sz, _sz, _sz, _u8p, _int, _intp, _vp]),
+    "rs8_reconstruct_batch_noalloc_limit": (_sz, [_sz, _sz, _sz]),
     "rs_batch_create": (_int, [_vp, _sz, _int, _intp, _pp]),
     "rs_batch_launch": (_int, [_vp, _vp]),
     "rs_batch_stats": (_int, [_vp, _szp, _szp, _szp, ctypes.POINTER(ctypes.c_uint64)]),

@@ -37,6 +37,7 @@ ERROR_NAMES = {
     103: "NoDevice",
     104: "Timeout",
     105: "LengthMismatch",
+    106: "TooLarge",
 }
 
 

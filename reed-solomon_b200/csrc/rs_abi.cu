@@ -290,6 +290,7 @@ const char *rs_strerror(int status) {
     case RS_ERR_NO_DEVICE: return "No usable CUDA device";
     case RS_ERR_TIMEOUT: return "A bounded device wait timed out";
     case RS_ERR_LENGTH_MISMATCH: return "Input and output lengths differ";
+    case RS_ERR_TOO_LARGE: return "The request needs more than the fixed working area holds";
     default: return "Unknown status";
   }
 }
