@@ -220,6 +220,73 @@ int rs_batch_stats(const rs_batch_t *batch, size_t *launches, size_t *fft_items,
                    size_t *matrix_items, uint64_t *bytes);
 void rs_batch_free(rs_batch_t *batch);
 
+/* ---- request server: continuous batching on one GPU ----
+ * No counterpart in the reference (a caller there runs one encode or reconstruct per
+ * call on its own thread). A server owns a device arena, a set of streams and a
+ * scheduler thread. Submitted requests wait in a FIFO queue and are admitted while a
+ * slot is free and their working set fits in the arena: the staged payload
+ * (host-memory requests), descriptors and decode rows, plus the generator table of
+ * their shape unless it is already resident. Tables stay resident across requests and
+ * idle ones are evicted, least recently used first, when space is needed. Every
+ * completion frees its memory and slot, so new work is admitted while older work is
+ * still running. GF(2^8) requests admitted together share one launch group (one FFT
+ * launch per (K,K) shape, one ragged matrix launch for the rest); GF(2^16) requests
+ * run one per group; groups overlap on the server's streams. Results are the bytes
+ * the single-stripe entry points produce. */
+typedef struct {
+  int field;                /* 8: ReedSolomon (k+m <= 256), 16: ReedSolomon16 (<= 65536) */
+  int op;                   /* enum rs_batch_op */
+  size_t data_shards;       /* k */
+  size_t parity_shards;     /* m */
+  size_t row_len;           /* shard bytes (even for field 16: low plane, then high) */
+  uint8_t *rows;            /* k+m rows of row_len bytes back to back, data first */
+  int rows_on_host;         /* 1: host memory, staged through the arena (pin it for
+                               overlap); 0: device memory the caller keeps alive */
+  const uint8_t *present;   /* k+m flags, reconstruct ops; copied at submit */
+  uint64_t tag;             /* returned in the completion */
+} rs_request;
+typedef struct {
+  uint64_t tag;
+  int status;               /* 0 or a reference error / device error */
+  uint32_t group_size;      /* requests in its launch group (0: nothing to do) */
+  uint64_t submit_ns, admit_ns, done_ns; /* host steady clock */
+  uint64_t bytes;           /* algorithmic bytes: (k+m)*len encode, (k+e)*len rebuild */
+} rs_completion;
+typedef struct {
+  size_t arena_bytes;       /* device working memory (0: 1 GiB) */
+  size_t pinned_bytes;      /* pinned host staging for descriptors (0: 64 MiB) */
+  int slots;                /* requests in flight at most (0: 64) */
+  int streams;              /* device streams (0: 4) */
+  int max_batch;            /* GF(2^8) requests per launch group (0: 64) */
+  int lookahead;            /* queued requests that may pass a head that does not fit */
+} rs_server_config;
+typedef struct {
+  uint64_t submitted, completed, rejected;
+  uint64_t groups, launches, merged; /* merged: requests that shared a group */
+  uint64_t bytes;                    /* algorithmic bytes of completed requests */
+  uint64_t table_builds, table_hits, evictions;
+  size_t arena_bytes, arena_used, arena_peak;
+  size_t queued, in_flight, resident_tables;
+} rs_server_stats;
+typedef struct rs_server rs_server_t;
+/* RS_ERR_TOO_LARGE when the arena cannot be allocated with 256 MiB to spare. */
+int rs_server_create(const rs_server_config *config, rs_server_t **out);
+/* Validates and queues n requests; statuses[i] (optional) is the request's reference
+ * error (as its single-stripe call would return it) or RS_ERR_TOO_LARGE when it can
+ * never fit the arena. Rejected requests produce no completion; a reconstruct with
+ * nothing to rebuild completes at once. Never blocks on the device. */
+int rs_server_submit(rs_server_t *server, const rs_request *reqs, size_t n, int *statuses);
+/* Moves up to cap completions into out; waits up to timeout_ms (-1: until one
+ * arrives, 0: no wait) when none is ready. */
+int rs_server_poll(rs_server_t *server, rs_completion *out, size_t cap, size_t *n_out,
+                   int timeout_ms);
+/* Route of (K,K) GF(2^8) encodes of 2^log2_bytes..2^(log2_bytes+1)-1 byte shards:
+ * 0 automatic (FFT from 64 bytes), 1 matrix, 2 FFT. Set from the cost model. */
+int rs_server_set_fft_route(rs_server_t *server, size_t k, int log2_bytes, int route);
+int rs_server_stats_get(rs_server_t *server, rs_server_stats *out);
+/* Waits for admitted work, drops requests still queued, frees everything. */
+void rs_server_free(rs_server_t *server);
+
 /* ========================= ReedSolomon16 (GF((2^8)^2)) ========================= */
 
 /* ReedSolomon16::new, src/reedsolomon16.rs:281-319 (k + m <= 65536). */

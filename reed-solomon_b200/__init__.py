@@ -23,3 +23,4 @@ from .coder import (  # noqa: F401
     mul_slice_xor,
 )
 from ._lib import LIB_PATH, load  # noqa: F401
+from .server import Server  # noqa: F401

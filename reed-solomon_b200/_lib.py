@@ -65,6 +65,12 @@ SIGNATURES = {
     "rs_batch_launch": (_int, [_vp, _vp]),
     "rs_batch_stats": (_int, [_vp, _szp, _szp, _szp, ctypes.POINTER(ctypes.c_uint64)]),
     "rs_batch_free": (None, [_vp]),
+    "rs_server_create": (_int, [_vp, _pp]),
+    "rs_server_submit": (_int, [_vp, _vp, _sz, _intp]),
+    "rs_server_poll": (_int, [_vp, _vp, _sz, _szp, _int]),
+    "rs_server_set_fft_route": (_int, [_vp, _sz, _int, _int]),
+    "rs_server_stats_get": (_int, [_vp, _vp]),
+    "rs_server_free": (None, [_vp]),
     "rs16_new": (_int, [_sz, _sz, _pp]),
     "rs16_clone": (_int, [_vp, _pp]),
     "rs16_free": (None, [_vp]),
