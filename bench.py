@@ -12,6 +12,14 @@ the public host-pointer API from pinned host memory, and the CPU baseline (the o
 multi-threaded restatement of the reference's GFNI FFT path).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Other workloads (one JSON line each, 1 GPU, no reference arm):
+    --workload stripes   RS(32,32) and RS(16,16) encode (FFT and matrix routes) and
+                         reconstruct, 4 KiB / 64 KiB / 1 MiB shards, 4096 stripes
+    --workload mixed     10,000 stripes of nine shapes, 25% reconstruct: batched+tuned
+                         (graph) against one plain launch per stripe
+    --workload rs16      ReedSolomon16 (1024,1024) and (4096,12288), 2 KiB shards
+    --workload serve     Poisson request stream at 50k req/s through the request server
 """
 import argparse
 import json
@@ -40,6 +48,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--stripes", type=int, default=1024, help="stripes per step per GPU")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--workload", default="encode", choices=["encode", "stripes", "mixed", "rs16", "serve"])
+    ap.add_argument("--requests", type=int, default=400, help="requests of the serve workload")
     return ap.parse_args()
 
 
@@ -281,8 +291,49 @@ def run_ours(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def run_workload(args):
+    """The non-headline workloads: one JSON line with the workload's results."""
+    import torch
+
+    import __graft_entry__
+
+    rsb = __graft_entry__.load_package()
+    torch.cuda.set_device(0)
+    from reed_solomon_b200 import workloads
+
+    hbm, hbm_kind = peaks()
+    launches0 = rsb.kernel_launch_count()
+    with Clocks(0) as clk:
+        if args.workload == "stripes":
+            res = workloads.stripes_sweep()
+            line = {"metric": "RS(k,k) encode/reconstruct GB/s, 4096 stripes per launch", "unit": "GB/s",
+                    "results": res}
+        elif args.workload == "mixed":
+            res = workloads.mixed_batch()
+            line = {"metric": "mixed-shape batch GB/s, batched+tuned vs plain", "unit": "GB/s",
+                    "value": res["batched_gbs"], "results": res}
+        elif args.workload == "rs16":
+            res = workloads.rs16_shapes()
+            line = {"metric": "ReedSolomon16 encode/reconstruct GB/s", "unit": "GB/s", "results": res}
+        else:
+            res = workloads.serve_poisson(count=args.requests)
+            line = {"metric": "request server p50/p99 latency and GB/s, Poisson 50k req/s", "unit": "GB/s",
+                    "value": res["gbs"], "results": res}
+    line.update({"workload": args.workload, "n_gpus": 1, "data": "synthetic (seeded uniform bytes, on device)",
+                 "hbm_peak_gbs": hbm, "hbm_peak_source": hbm_kind,
+                 "gpu_launches": rsb.kernel_launch_count() - launches0, "clocks": clk.summary()})
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload != "encode":
+        if args.impl == "reference" or int(os.environ.get("WORLD_SIZE", 1)) > 1:
+            print(json.dumps({"impl": args.impl, "workload": args.workload,
+                              "unavailable": "workload runs on one GPU, our implementation only"}))
+            return
+        run_workload(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", 1))
     rank = int(os.environ.get("RANK", 0))
     if world > 1 and args.impl == "ours":

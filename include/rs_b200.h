@@ -320,8 +320,13 @@ int rs16_dec_reconstruct(rs16_dec_t *dec, uint8_t *const *shards, const size_t *
                          const uint8_t *present, size_t n_shards, int data_only);
 int rs16_dec_clone(const rs16_dec_t *dec, rs16_dec_t **out);
 void rs16_dec_free(rs16_dec_t *dec);
-/* ReedSolomon16::encode_route, src/reedsolomon16.rs:335-346: "matrix". */
+/* ReedSolomon16::encode_route, src/reedsolomon16.rs:335-346: "fft" (bitsliced tower
+ * LCH transform, src/fft16.rs; k a power of two, any m, picked when its estimated work
+ * is below the matrix kernel's) or "matrix". */
 const char *rs16_encode_route(const rs16_t *codec);
+/* Forced-route test hook like rs8_set_route: 0 automatic, 1 matrix, 2 FFT where the
+ * shape has it (k a power of two >= 2). Both routes give identical bytes. */
+int rs16_set_route(rs16_t *codec, int route);
 int rs16_encode_dev(rs16_t *codec, uint8_t *const *d_shards, size_t n_shards, size_t len,
                     void *stream);
 /* Many stripes of one shape: stripe s reads k rows at d_data + s*data_stride and

@@ -340,6 +340,10 @@ class ReedSolomon16(_Coder):
     def encode_route(self):
         return self._L.rs16_encode_route(self._h).decode()
 
+    def set_route(self, route):
+        """Test hook: "auto", "matrix" or "fft" (identical bytes on every route)."""
+        _check(self._L.rs16_set_route(self._h, {"auto": 0, "matrix": 1, "fft": 2}[route]))
+
     def encode(self, shards):
         arrs = [_as_u8(s, i >= self._k) for i, s in enumerate(shards)]
         if len(arrs) == self.total_shard_count():

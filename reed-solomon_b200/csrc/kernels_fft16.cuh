@@ -1,0 +1,211 @@
+// FFT-route encode for ReedSolomon16: the Lin-Chung-Han additive FFT over the tower
+// field GF((2^8)^2) (src/fft16.rs), bitsliced for CUDA cores.
+//
+// For k = K a power of two, encode is an inverse transform of the K data rows on the
+// points {0..K-1} (interpolation into the novel basis, src/fft16.rs:223-) followed,
+// for every coset {cK .. cK+K-1} that holds parity points, by a forward transform of
+// those coefficients with beta = cK; the outputs are the parity rows in point order.
+// Butterflies follow the reference's order and constants: at level l a block of
+// 2^(l+1) registers at `base` uses c = WHAT[l][beta ^ base]; inverse: hi ^= lo,
+// lo ^= c*hi; forward: lo ^= c*hi, hi ^= lo.
+//
+// Bitslicing. 32 symbols of one shard (32 low-plane bytes and 32 high-plane bytes)
+// become 16 bit planes: planes 0..7 hold the low byte's bits, 8..15 the high byte's,
+// so bit p of a symbol's u16 value is plane p. Multiplying by a constant c is the
+// 16x16 GF(2) matrix whose column p is c * 2^p: plane b of the product is the XOR of
+// the planes p with bit b of c * 2^p set. The constants differ per butterfly block and
+// are only known at run time, so the matrix is applied as 256 masked XORs (one
+// three-input LOP3 each) with masks in shared memory.
+//
+// Work split. The transform runs over a bitsliced scratch buffer, word
+// ((s * R + r) * G + g) * 16 + p for stripe s, register r of R, 32-symbol group g of G.
+// A pass applies one or two levels: a CTA (a multiple of 32 threads, at most 256) owns
+// one butterfly group (2 or 4 registers) and its warps take (stripe, 32 groups) tasks, one lane per 32-symbol group, so every
+// lane of a CTA uses the same constants and reads their masks as shared-memory
+// broadcasts.
+#pragma once
+
+#include <cstdint>
+
+#include "kernels_fft.cuh"
+
+namespace rsb {
+
+constexpr int kFft16Threads = 256;
+
+struct Fft16PassArgs {
+  const uint32_t *src;
+  uint32_t *dst;
+  const uint16_t *cols;  // per constant: 16 columns c * 2^p; constant (l, j) at R - (R >> l) + j
+  uint32_t R;            // registers in the transform (a power of two)
+  uint32_t level;        // lowest level of the pass
+  uint64_t G;            // 32-symbol groups per shard
+  uint32_t n_stripes;
+  int inverse;
+};
+
+using Reg16 = uint32_t[16];
+
+// d ^= M * s, M as masks m[b * 16 + p] (all-ones when bit b of c * 2^p is set).
+__device__ __forceinline__ void mul16_acc(Reg16 &d, const Reg16 &s, const uint32_t *m) {
+#pragma unroll
+  for (int b = 0; b < 16; b++) {
+    const uint4 *m4 = reinterpret_cast<const uint4 *>(m + b * 16);
+    uint32_t acc = d[b];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const uint4 v = m4[q];
+      acc ^= s[4 * q] & v.x;
+      acc ^= s[4 * q + 1] & v.y;
+      acc ^= s[4 * q + 2] & v.z;
+      acc ^= s[4 * q + 3] & v.w;
+    }
+    d[b] = acc;
+  }
+}
+
+__device__ __forceinline__ void xor16(Reg16 &d, const Reg16 &s) {
+#pragma unroll
+  for (int p = 0; p < 16; p++) d[p] ^= s[p];
+}
+
+// inverse: hi ^= lo, lo ^= c*hi; forward: lo ^= c*hi, hi ^= lo.
+__device__ __forceinline__ void bfly16(Reg16 &lo, Reg16 &hi, const uint32_t *m, bool inverse) {
+  if (inverse) {
+    xor16(hi, lo);
+    mul16_acc(lo, hi, m);
+  } else {
+    mul16_acc(lo, hi, m);
+    xor16(hi, lo);
+  }
+}
+
+__device__ __forceinline__ void load_reg16(const uint32_t *p, Reg16 &r) {
+  const uint4 *q = reinterpret_cast<const uint4 *>(p);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    uint4 v = q[i];
+    r[4 * i] = v.x, r[4 * i + 1] = v.y, r[4 * i + 2] = v.z, r[4 * i + 3] = v.w;
+  }
+}
+
+__device__ __forceinline__ void store_reg16(uint32_t *p, const Reg16 &r) {
+  uint4 *q = reinterpret_cast<uint4 *>(p);
+#pragma unroll
+  for (int i = 0; i < 4; i++) q[i] = make_uint4(r[4 * i], r[4 * i + 1], r[4 * i + 2], r[4 * i + 3]);
+}
+
+// LV = 1: registers {i0, i0+h} at level L (h = 2^L). LV = 2: {i0, i0+h, i0+2h, i0+3h},
+// levels L and L+1 (inverse: L then L+1; forward: L+1 then L).
+template <int LV>
+__global__ void __launch_bounds__(kFft16Threads) fft16_pass_kernel(const Fft16PassArgs a) {
+  constexpr int NC = LV == 2 ? 3 : 1;
+  __shared__ __align__(16) uint32_t mk[NC][256];
+  const uint32_t R = a.R, L = a.level, h = 1u << L;
+  const uint32_t grp = blockIdx.x;
+  const uint32_t blk = grp >> L, i = grp & (h - 1);
+  const uint32_t i0 = blk * (h << LV) + i;
+  uint32_t cidx[NC];
+  if constexpr (LV == 2) {
+    cidx[0] = R - (R >> L) + 2 * blk;          // level L, block of i0 / i0+h
+    cidx[1] = R - (R >> L) + 2 * blk + 1;      // level L, block of i0+2h / i0+3h
+    cidx[2] = R - (R >> (L + 1)) + blk;        // level L+1
+  } else {
+    cidx[0] = R - (R >> L) + blk;
+  }
+  for (uint32_t t = threadIdx.x; t < NC * 256; t += blockDim.x) {
+    const uint32_t c = t >> 8, b = (t >> 4) & 15, p = t & 15;
+    mk[c][t & 255] = ((a.cols[16 * cidx[c] + p] >> b) & 1) ? ~0u : 0u;
+  }
+  __syncthreads();
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+  const uint64_t chunks = (a.G + 31) / 32;
+  const uint64_t tasks = (uint64_t)a.n_stripes * chunks;
+  for (uint64_t task = (uint64_t)blockIdx.y * warps + warp; task < tasks; task += (uint64_t)gridDim.y * warps) {
+    const uint64_t s = task / chunks;
+    const uint64_t g = (task % chunks) * 32 + lane;
+    if (g >= a.G) continue;
+    const uint64_t base = s * R;
+    auto word = [&](uint32_t r) { return ((base + r) * a.G + g) * 16; };
+    if constexpr (LV == 2) {
+      Reg16 r0, r1, r2, r3;
+      load_reg16(a.src + word(i0), r0);
+      load_reg16(a.src + word(i0 + h), r1);
+      load_reg16(a.src + word(i0 + 2 * h), r2);
+      load_reg16(a.src + word(i0 + 3 * h), r3);
+      if (a.inverse) {
+        bfly16(r0, r1, mk[0], true);
+        bfly16(r2, r3, mk[1], true);
+        bfly16(r0, r2, mk[2], true);
+        bfly16(r1, r3, mk[2], true);
+      } else {
+        bfly16(r0, r2, mk[2], false);
+        bfly16(r1, r3, mk[2], false);
+        bfly16(r0, r1, mk[0], false);
+        bfly16(r2, r3, mk[1], false);
+      }
+      store_reg16(a.dst + word(i0), r0);
+      store_reg16(a.dst + word(i0 + h), r1);
+      store_reg16(a.dst + word(i0 + 2 * h), r2);
+      store_reg16(a.dst + word(i0 + 3 * h), r3);
+    } else {
+      Reg16 r0, r1;
+      load_reg16(a.src + word(i0), r0);
+      load_reg16(a.src + word(i0 + h), r1);
+      bfly16(r0, r1, mk[0], a.inverse != 0);
+      store_reg16(a.dst + word(i0), r0);
+      store_reg16(a.dst + word(i0 + h), r1);
+    }
+  }
+}
+
+// Shard bytes -> bit planes: row r of stripe s (low plane [0,N), high plane [N,2N))
+// into scratch register r; symbols past N read as zero. Rows are strided, or (one
+// stripe) taken from the device pointer table in_ptrs.
+__global__ void __launch_bounds__(kFft16Threads)
+    fft16_load_kernel(const uint8_t *in_base, uint64_t in_row, uint64_t in_stripe, const uint8_t *const *in_ptrs,
+                      uint32_t rows, uint64_t N, uint64_t G, uint32_t n_stripes, uint32_t R, uint32_t *dst) {
+  const uint64_t total = (uint64_t)n_stripes * rows * G;
+  for (uint64_t t = (uint64_t)blockIdx.x * kFft16Threads + threadIdx.x; t < total;
+       t += (uint64_t)gridDim.x * kFft16Threads) {
+    const uint64_t g = t % G, sr = t / G;
+    const uint64_t r = sr % rows, s = sr / rows;
+    const uint8_t *row = in_ptrs ? in_ptrs[r] : in_base + s * in_stripe + r * in_row;
+    const uint64_t col = g * 32, remain = N - col;
+    uint32_t lo[8], hi[8];
+    load32(row + col, remain, lo);
+    load32(row + N + col, remain, hi);
+    bit_transpose(lo);
+    bit_transpose(hi);
+    uint4 *q = reinterpret_cast<uint4 *>(dst + ((s * R + r) * G + g) * 16);
+    q[0] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    q[1] = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+    q[2] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    q[3] = make_uint4(hi[4], hi[5], hi[6], hi[7]);
+  }
+}
+
+// Bit planes -> shard bytes: scratch registers [0, rows) of each stripe into output
+// rows out_base + s * out_stripe + r * out_row, or (one stripe) out_ptrs[r].
+__global__ void __launch_bounds__(kFft16Threads)
+    fft16_store_kernel(const uint32_t *src, uint32_t R, uint32_t rows, uint64_t N, uint64_t G, uint32_t n_stripes,
+                       uint8_t *out_base, uint64_t out_row, uint64_t out_stripe, uint8_t *const *out_ptrs) {
+  const uint64_t total = (uint64_t)n_stripes * rows * G;
+  for (uint64_t t = (uint64_t)blockIdx.x * kFft16Threads + threadIdx.x; t < total;
+       t += (uint64_t)gridDim.x * kFft16Threads) {
+    const uint64_t g = t % G, sr = t / G;
+    const uint64_t r = sr % rows, s = sr / rows;
+    const uint4 *q = reinterpret_cast<const uint4 *>(src + ((s * R + r) * G + g) * 16);
+    uint4 a = q[0], b = q[1], c = q[2], d = q[3];
+    uint32_t lo[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    uint32_t hi[8] = {c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w};
+    bit_transpose(lo);
+    bit_transpose(hi);
+    uint8_t *row = out_ptrs ? out_ptrs[r] : out_base + s * out_stripe + r * out_row;
+    const uint64_t col = g * 32, remain = N - col;
+    store32(row + col, remain, lo);
+    store32(row + N + col, remain, hi);
+  }
+}
+
+}  // namespace rsb
