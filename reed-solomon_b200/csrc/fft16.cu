@@ -1,0 +1,282 @@
+// Host side of the ReedSolomon16 FFT route: program construction (fft16.hpp) and the
+// launch sequence of one run.
+#include "fft16.hpp"
+
+#include <algorithm>
+
+#include "gf_host.hpp"
+#include "kernels_fft16.cuh"
+#include "runtime.hpp"
+
+namespace rsb {
+
+namespace {
+
+// WHAT[l][x] of the tower field: W_0(x) = x, W_{j+1}(x) = W_j(x) (W_j(x) + W_j(2^j)),
+// each level scaled so that W_l(2^l) = 1 (src/fft16.rs:42-70). Evaluated per point by
+// running the recurrence, which needs the unscaled pivots W_j(2^j).
+struct What16 {
+  uint16_t pivot[16], pivot_inv[16];
+  What16() {
+    for (int l = 0; l < 16; l++) {
+      pivot[l] = raw(l, (uint16_t)(1u << l));
+      pivot_inv[l] = gf16_inv(pivot[l]);
+    }
+  }
+  uint16_t raw(int l, uint16_t x) const {
+    uint16_t w = x;
+    for (int j = 0; j < l; j++) w = gf16_mul(w, (uint16_t)(w ^ pivot[j]));
+    return w;
+  }
+  uint16_t operator()(int l, uint16_t x) const { return gf16_mul(raw(l, x), pivot_inv[l]); }
+};
+
+const What16 &what16() {
+  static const What16 w;
+  return w;
+}
+
+int log2_exact(uint64_t x) {
+  int l = 0;
+  while ((1ull << l) < x) l++;
+  return l;
+}
+
+uint64_t push_const(Fft16Program &p, uint16_t c) {
+  uint64_t at = p.cols.size() / 16;
+  for (int b = 0; b < 16; b++) p.cols.push_back(gf16_mul(c, (uint16_t)(1u << b)));
+  return at;
+}
+
+// Constants of a transform of `size` registers at `beta`: (l, j) at size - (size >> l) + j.
+uint64_t push_transform(Fft16Program &p, uint32_t size, uint32_t beta) {
+  uint64_t at = p.cols.size() / 16;
+  const int lg = log2_exact(size);
+  for (int l = 0; l < lg; l++)
+    for (uint32_t j = 0; j < (size >> (l + 1)); j++) push_const(p, what16()(l, (uint16_t)(beta ^ (j << (l + 1)))));
+  p.butterflies += (uint64_t)(size / 2) * lg;
+  return at;
+}
+
+void transform(Fft16Program &p, uint8_t src_buf, uint32_t src_start, uint8_t dst_buf, uint32_t dst_start,
+               uint32_t size, uint32_t beta, bool inverse) {
+  Fft16Step s{};
+  s.kind = Fft16Step::kTransform;
+  s.src_buf = src_buf;
+  s.dst_buf = dst_buf;
+  s.src_start = src_start;
+  s.dst_start = dst_start;
+  s.size = size;
+  s.inverse = inverse;
+  s.cols = push_transform(p, size, beta);
+  p.interp.push_back(s);
+}
+
+void mulxor(Fft16Program &p, uint8_t src_buf, uint32_t src_start, uint32_t dst_start, uint32_t count, uint16_t c) {
+  if (c == 0 || count == 0) return;
+  Fft16Step s{};
+  s.kind = Fft16Step::kMulXor;
+  s.src_buf = src_buf;
+  s.dst_buf = 0;
+  s.src_start = src_start;
+  s.dst_start = dst_start;
+  s.size = count;
+  s.cols = c == 1 ? Fft16Program::kNoConst : push_const(p, c);
+  p.butterflies += count;
+  p.interp.push_back(s);
+}
+
+// Builder::interpolate (src/fft.rs:198-239) on C registers [start, start+n): the first k
+// hold values at beta + 0 .. beta + k-1; afterwards they hold the novel-basis
+// coefficients (the rest stay zero).
+void interpolate(Fft16Program &p, uint32_t start, uint32_t n, uint32_t beta, uint32_t k) {
+  if (k == n) {
+    if (n > 1) transform(p, 0, start, 0, start, n, beta, true);
+    return;
+  }
+  const uint32_t half = n / 2;
+  if (k <= half) {
+    interpolate(p, start, half, beta, k);
+    return;
+  }
+  if (half > 1) transform(p, 0, start, 0, start, half, beta, true);
+  const uint16_t c = what16()(log2_exact(n) - 1, (uint16_t)beta);
+  // Evaluate the first half's polynomial on the second half's points (in S), subtract.
+  if (half > 1) {
+    transform(p, 0, start, 1, 0, half, beta ^ half, false);
+    mulxor(p, 1, 0, start + half, k - half, 1);
+  } else {
+    mulxor(p, 0, start, start + half, k - half, 1);
+  }
+  interpolate(p, start + half, half, beta ^ half, k - half);
+  mulxor(p, 0, start + half, start, k - half, c);
+}
+
+}  // namespace
+
+bool fft16_build(size_t k, size_t m, Fft16Program &p) {
+  if (k < 2 || m == 0 || k + m > 65536) return false;
+  p = Fft16Program{};
+  p.k = (uint32_t)k;
+  p.m = (uint32_t)m;
+  uint32_t t = 1;
+  while (t < k) t <<= 1;
+  p.t = t;
+  interpolate(p, 0, t, 0, (uint32_t)k);
+  const uint64_t n = k + m;
+  for (uint64_t beta = 0; beta < n; beta += t) {
+    const uint64_t lo = std::max<uint64_t>(k, beta), hi = std::min<uint64_t>(n, beta + t);
+    if (lo >= hi) continue;
+    Fft16Eval e{};
+    e.beta = (uint32_t)beta;
+    e.cols = push_transform(p, t, (uint32_t)beta);
+    e.r_lo = (uint32_t)(lo - beta);
+    e.r_hi = (uint32_t)(hi - beta);
+    e.parity_row = lo - k;
+    p.evals.push_back(e);
+  }
+  return true;
+}
+
+bool fft16_preferred(const Fft16Program &p) {
+  // LOP3 per 32-symbol group: the matrix kernel about 208 per coefficient, a butterfly
+  // about 290; the FFT's passes also move scratch through L2 (counted as 2x).
+  const double fft = 2.0 * 290.0 * (double)p.butterflies + 64.0 * p.regs();
+  const double matrix = 208.0 * (double)p.k * p.m;
+  return fft < matrix;
+}
+
+size_t fft16_scratch_bytes(const Fft16Program &p, size_t n_stripes, size_t len, size_t budget) {
+  const uint64_t G = (len / 2 + 31) / 32, per_group = (uint64_t)p.regs() * 64;
+  const uint64_t all = (uint64_t)n_stripes * G * per_group;
+  return (size_t)std::max<uint64_t>(per_group, std::min<uint64_t>(all, budget / per_group * per_group));
+}
+
+int fft16_run(const Fft16Program &p, const uint16_t *d_cols, uint8_t *scratch, size_t scratch_bytes,
+              const uint8_t *in_base, uint64_t in_row, uint64_t in_stripe, uint8_t *out_base, uint64_t out_row,
+              uint64_t out_stripe, uint8_t *const *d_ptrs, size_t n_stripes, size_t len, cudaStream_t st) {
+  const uint32_t t = p.t, k = p.k;
+  const uint64_t N = len / 2, G = (N + 31) / 32, per_group = (uint64_t)p.regs() * 64;
+  if (scratch_bytes < per_group) return RS_ERR_TOO_LARGE;
+  // A unit of work: `wave` stripes x `gc` groups.
+  uint64_t wave, gc;
+  if (G * per_group <= scratch_bytes) {
+    gc = G;
+    wave = std::max<uint64_t>(1, std::min<uint64_t>(n_stripes, scratch_bytes / (G * per_group)));
+  } else {
+    wave = 1;
+    gc = scratch_bytes / per_group;
+  }
+  const uint32_t regs_of[3] = {t, std::max<uint32_t>(1, t / 2), t};
+  auto grid_for = [](uint64_t items) {
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((items + kFft16Threads - 1) / kFft16Threads, 148 * 16));
+  };
+  for (uint64_t s0 = 0; s0 < n_stripes; s0 += wave) {
+    const uint32_t ns = (uint32_t)std::min<uint64_t>(wave, n_stripes - s0);
+    for (uint64_t g0 = 0; g0 < G; g0 += gc) {
+      const uint64_t gn = std::min<uint64_t>(gc, G - g0);
+      uint32_t *buf[3];
+      buf[0] = reinterpret_cast<uint32_t *>(scratch);
+      buf[1] = buf[0] + (uint64_t)ns * regs_of[0] * gn * 16;
+      buf[2] = buf[1] + (uint64_t)ns * regs_of[1] * gn * 16;
+      auto pass = [&](const Fft16Step &s, const uint32_t *src, uint32_t src_regs, uint32_t src_start, int level,
+                      int lv) -> int {
+        Fft16PassArgs a{};
+        a.src = src;
+        a.dst = buf[s.dst_buf];
+        a.cols = d_cols + s.cols * 16;
+        a.R = s.size;
+        a.level = (uint32_t)level;
+        a.src_regs = src_regs;
+        a.src_start = src_start;
+        a.dst_regs = regs_of[s.dst_buf];
+        a.dst_start = s.dst_start;
+        a.G = gn;
+        a.n_stripes = ns;
+        a.inverse = s.inverse;
+        const uint64_t tasks = (uint64_t)ns * ((gn + 31) / 32);
+        const unsigned threads = (unsigned)(32 * std::min<uint64_t>(8, tasks));
+        const unsigned gy = (unsigned)std::min<uint64_t>(65535, (tasks * 32 + threads - 1) / threads);
+        if (lv == 2)
+          fft16_pass_kernel<2><<<dim3(s.size / 4, gy), threads, 0, st>>>(a);
+        else
+          fft16_pass_kernel<1><<<dim3(s.size / 2, gy), threads, 0, st>>>(a);
+        g_launches++;
+        RSB_CU(cudaGetLastError());
+        return RS_OK;
+      };
+      // Levels of a transform: inverse 0, 1 | 2, 3 | ... (an odd top level alone, last);
+      // forward the mirror image. The first pass reads the source window.
+      auto run_transform = [&](const Fft16Step &s) -> int {
+        const int lg = log2_exact(s.size);
+        const uint32_t *src = buf[s.src_buf];
+        uint32_t src_regs = regs_of[s.src_buf], src_start = s.src_start;
+        auto advance = [&]() {
+          src = buf[s.dst_buf];
+          src_regs = regs_of[s.dst_buf];
+          src_start = s.dst_start;
+        };
+        if (s.inverse) {
+          int L = 0;
+          for (; L + 1 < lg; L += 2) {
+            RSB_TRY(pass(s, src, src_regs, src_start, L, 2));
+            advance();
+          }
+          if (L < lg) RSB_TRY(pass(s, src, src_regs, src_start, L, 1));
+        } else {
+          int top = lg - 1;
+          if (lg % 2 == 1) {
+            RSB_TRY(pass(s, src, src_regs, src_start, top, 1));
+            advance();
+            top--;
+          }
+          for (int l = top - 1; l >= 0; l -= 2) {
+            RSB_TRY(pass(s, src, src_regs, src_start, l, 2));
+            advance();
+          }
+        }
+        return RS_OK;
+      };
+      // Data into C[0, k); C[k, t) zero.
+      fft16_load_kernel<<<grid_for((uint64_t)ns * k * gn), kFft16Threads, 0, st>>>(
+          in_base + s0 * in_stripe, in_row, in_stripe, reinterpret_cast<const uint8_t *const *>(d_ptrs), k, N, g0,
+          gn, ns, t, buf[0]);
+      g_launches++;
+      RSB_CU(cudaGetLastError());
+      if (k < t)
+        RSB_CU(cudaMemset2DAsync(buf[0] + (uint64_t)k * gn * 16, (size_t)t * gn * 64, 0, (size_t)(t - k) * gn * 64,
+                                 ns, st));
+      for (const Fft16Step &s : p.interp) {
+        if (s.kind == Fft16Step::kTransform) {
+          RSB_TRY(run_transform(s));
+          continue;
+        }
+        const uint64_t items = (uint64_t)ns * s.size * gn;
+        fft16_mulxor_kernel<<<grid_for(items), kFft16Threads, 0, st>>>(
+            buf[s.src_buf], regs_of[s.src_buf], s.src_start, buf[0], regs_of[0], s.dst_start, s.size, gn, ns,
+            s.cols == Fft16Program::kNoConst ? nullptr : d_cols + s.cols * 16);
+        g_launches++;
+        RSB_CU(cudaGetLastError());
+      }
+      for (const Fft16Eval &e : p.evals) {
+        Fft16Step s{};
+        s.kind = Fft16Step::kTransform;
+        s.src_buf = 0;
+        s.dst_buf = 2;
+        s.size = t;
+        s.cols = e.cols;
+        RSB_TRY(run_transform(s));
+        const uint32_t rows = e.r_hi - e.r_lo;
+        fft16_store_kernel<<<grid_for((uint64_t)ns * rows * gn), kFft16Threads, 0, st>>>(
+            buf[2] + (uint64_t)e.r_lo * gn * 16, t, rows, N, g0, gn, ns,
+            d_ptrs ? nullptr : out_base + s0 * out_stripe + e.parity_row * out_row, out_row, out_stripe,
+            d_ptrs ? d_ptrs + k + e.parity_row : nullptr);
+        g_launches++;
+        RSB_CU(cudaGetLastError());
+      }
+    }
+  }
+  return RS_OK;
+}
+
+}  // namespace rsb

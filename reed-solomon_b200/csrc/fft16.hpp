@@ -1,0 +1,63 @@
+// FFT-route encode of ReedSolomon16 for any k >= 2 (src/fft16.rs): a step program built
+// once per shape on the host and run by the kernels of kernels_fft16.cuh.
+//
+// Program. With t the power of two >= k, interpolation through the k data points
+// follows the reference's recursion (src/fft.rs:198-239, the tower builder of
+// src/fft16.rs:223-): an inverse transform where a whole half of the points is known;
+// otherwise the known first half is interpolated, evaluated on the second half's points
+// and subtracted, the rest interpolated recursively, and the halves combined with the
+// constant WHAT[level][beta]. Evaluation then runs one forward transform of the t
+// coefficients per coset {c*t .. c*t+t-1} holding parity points (c = 0 included when
+// k < t). The registers live in three bitsliced buffers per stripe: C (t registers: the
+// data, then the coefficients), S (t/2: interpolation scratch) and W (t: evaluation).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+namespace rsb {
+
+struct Fft16Step {
+  enum Kind : uint8_t { kTransform, kMulXor } kind;
+  uint8_t src_buf, dst_buf;  // 0 = C, 1 = S, 2 = W
+  bool inverse;              // transform direction
+  uint32_t src_start, dst_start;
+  uint32_t size;             // transform: registers (a power of two); mulxor: count
+  uint64_t cols;             // first constant of the transform, or the mulxor constant;
+                             // kNoConst: plain XOR
+};
+
+struct Fft16Eval {
+  uint32_t beta;        // coset of the forward transform W = FFT(C)
+  uint64_t cols;        // its first constant
+  uint32_t r_lo, r_hi;  // W registers stored, as parity rows parity_row ...
+  uint64_t parity_row;
+};
+
+struct Fft16Program {
+  static constexpr uint64_t kNoConst = ~0ull;
+  uint32_t k = 0, m = 0, t = 0;
+  std::vector<Fft16Step> interp;
+  std::vector<Fft16Eval> evals;
+  std::vector<uint16_t> cols;  // 16 columns c * 2^p per constant
+  uint64_t butterflies = 0;    // per 32-symbol group (route estimate)
+  uint32_t regs() const { return t + t / 2 + t; }  // C + S + W per stripe and group
+};
+
+// False (no FFT route) for k < 2.
+bool fft16_build(size_t k, size_t m, Fft16Program &p);
+// Whether the FFT route's estimated work is below the tower matrix kernel's.
+bool fft16_preferred(const Fft16Program &p);
+// Scratch for one run: all stripes at once when that fits `budget`, else the largest
+// slice of one stripe's 32-symbol groups that does (at least one group).
+size_t fft16_scratch_bytes(const Fft16Program &p, size_t n_stripes, size_t len, size_t budget);
+// Encodes n_stripes stripes: data row r of stripe s at in_base + s*in_stripe + r*in_row,
+// parity row j at out_base + s*out_stripe + j*out_row; with d_ptrs (one stripe) the rows
+// are its k + m device pointers. All work is enqueued on `st`, using `scratch`.
+int fft16_run(const Fft16Program &p, const uint16_t *d_cols, uint8_t *scratch, size_t scratch_bytes,
+              const uint8_t *in_base, uint64_t in_row, uint64_t in_stripe, uint8_t *out_base, uint64_t out_row,
+              uint64_t out_stripe, uint8_t *const *d_ptrs, size_t n_stripes, size_t len, cudaStream_t st);
+
+}  // namespace rsb

@@ -33,13 +33,17 @@ namespace rsb {
 
 constexpr int kFft16Threads = 256;
 
+// A transform over a window of registers: it reads src registers [src_start, +R) and
+// writes dst registers [dst_start, +R) of buffers holding src_regs / dst_regs registers
+// per stripe (src may equal dst).
 struct Fft16PassArgs {
   const uint32_t *src;
   uint32_t *dst;
   const uint16_t *cols;  // per constant: 16 columns c * 2^p; constant (l, j) at R - (R >> l) + j
   uint32_t R;            // registers in the transform (a power of two)
   uint32_t level;        // lowest level of the pass
-  uint64_t G;            // 32-symbol groups per shard
+  uint32_t src_regs, src_start, dst_regs, dst_start;
+  uint64_t G;            // 32-symbol groups per shard in the buffers
   uint32_t n_stripes;
   int inverse;
 };
@@ -125,14 +129,15 @@ __global__ void __launch_bounds__(kFft16Threads) fft16_pass_kernel(const Fft16Pa
     const uint64_t s = task / chunks;
     const uint64_t g = (task % chunks) * 32 + lane;
     if (g >= a.G) continue;
-    const uint64_t base = s * R;
-    auto word = [&](uint32_t r) { return ((base + r) * a.G + g) * 16; };
+    const uint64_t sb = s * a.src_regs + a.src_start, db = s * a.dst_regs + a.dst_start;
+    auto sw = [&](uint32_t r) { return ((sb + r) * a.G + g) * 16; };
+    auto dw = [&](uint32_t r) { return ((db + r) * a.G + g) * 16; };
     if constexpr (LV == 2) {
       Reg16 r0, r1, r2, r3;
-      load_reg16(a.src + word(i0), r0);
-      load_reg16(a.src + word(i0 + h), r1);
-      load_reg16(a.src + word(i0 + 2 * h), r2);
-      load_reg16(a.src + word(i0 + 3 * h), r3);
+      load_reg16(a.src + sw(i0), r0);
+      load_reg16(a.src + sw(i0 + h), r1);
+      load_reg16(a.src + sw(i0 + 2 * h), r2);
+      load_reg16(a.src + sw(i0 + 3 * h), r3);
       if (a.inverse) {
         bfly16(r0, r1, mk[0], true);
         bfly16(r2, r3, mk[1], true);
@@ -144,34 +149,35 @@ __global__ void __launch_bounds__(kFft16Threads) fft16_pass_kernel(const Fft16Pa
         bfly16(r0, r1, mk[0], false);
         bfly16(r2, r3, mk[1], false);
       }
-      store_reg16(a.dst + word(i0), r0);
-      store_reg16(a.dst + word(i0 + h), r1);
-      store_reg16(a.dst + word(i0 + 2 * h), r2);
-      store_reg16(a.dst + word(i0 + 3 * h), r3);
+      store_reg16(a.dst + dw(i0), r0);
+      store_reg16(a.dst + dw(i0 + h), r1);
+      store_reg16(a.dst + dw(i0 + 2 * h), r2);
+      store_reg16(a.dst + dw(i0 + 3 * h), r3);
     } else {
       Reg16 r0, r1;
-      load_reg16(a.src + word(i0), r0);
-      load_reg16(a.src + word(i0 + h), r1);
+      load_reg16(a.src + sw(i0), r0);
+      load_reg16(a.src + sw(i0 + h), r1);
       bfly16(r0, r1, mk[0], a.inverse != 0);
-      store_reg16(a.dst + word(i0), r0);
-      store_reg16(a.dst + word(i0 + h), r1);
+      store_reg16(a.dst + dw(i0), r0);
+      store_reg16(a.dst + dw(i0 + h), r1);
     }
   }
 }
 
-// Shard bytes -> bit planes: row r of stripe s (low plane [0,N), high plane [N,2N))
-// into scratch register r; symbols past N read as zero. Rows are strided, or (one
-// stripe) taken from the device pointer table in_ptrs.
+// Shard bytes -> bit planes: row r of stripe s (low plane [0,N), high plane [N,2N)),
+// symbol groups g0 .. g0+G-1, into scratch register r; symbols past N read as zero.
+// Rows are strided, or (one stripe) taken from the device pointer table in_ptrs.
 __global__ void __launch_bounds__(kFft16Threads)
     fft16_load_kernel(const uint8_t *in_base, uint64_t in_row, uint64_t in_stripe, const uint8_t *const *in_ptrs,
-                      uint32_t rows, uint64_t N, uint64_t G, uint32_t n_stripes, uint32_t R, uint32_t *dst) {
+                      uint32_t rows, uint64_t N, uint64_t g0, uint64_t G, uint32_t n_stripes, uint32_t R,
+                      uint32_t *dst) {
   const uint64_t total = (uint64_t)n_stripes * rows * G;
   for (uint64_t t = (uint64_t)blockIdx.x * kFft16Threads + threadIdx.x; t < total;
        t += (uint64_t)gridDim.x * kFft16Threads) {
     const uint64_t g = t % G, sr = t / G;
     const uint64_t r = sr % rows, s = sr / rows;
     const uint8_t *row = in_ptrs ? in_ptrs[r] : in_base + s * in_stripe + r * in_row;
-    const uint64_t col = g * 32, remain = N - col;
+    const uint64_t col = (g0 + g) * 32, remain = N - col;
     uint32_t lo[8], hi[8];
     load32(row + col, remain, lo);
     load32(row + N + col, remain, hi);
@@ -185,11 +191,13 @@ __global__ void __launch_bounds__(kFft16Threads)
   }
 }
 
-// Bit planes -> shard bytes: scratch registers [0, rows) of each stripe into output
-// rows out_base + s * out_stripe + r * out_row, or (one stripe) out_ptrs[r].
+// Bit planes -> shard bytes: scratch registers [0, rows) of each stripe (R per stripe)
+// into symbol groups g0 .. g0+G-1 of output rows out_base + s * out_stripe + r * out_row,
+// or (one stripe) out_ptrs[r].
 __global__ void __launch_bounds__(kFft16Threads)
-    fft16_store_kernel(const uint32_t *src, uint32_t R, uint32_t rows, uint64_t N, uint64_t G, uint32_t n_stripes,
-                       uint8_t *out_base, uint64_t out_row, uint64_t out_stripe, uint8_t *const *out_ptrs) {
+    fft16_store_kernel(const uint32_t *src, uint32_t R, uint32_t rows, uint64_t N, uint64_t g0, uint64_t G,
+                       uint32_t n_stripes, uint8_t *out_base, uint64_t out_row, uint64_t out_stripe,
+                       uint8_t *const *out_ptrs) {
   const uint64_t total = (uint64_t)n_stripes * rows * G;
   for (uint64_t t = (uint64_t)blockIdx.x * kFft16Threads + threadIdx.x; t < total;
        t += (uint64_t)gridDim.x * kFft16Threads) {
@@ -202,9 +210,36 @@ __global__ void __launch_bounds__(kFft16Threads)
     bit_transpose(lo);
     bit_transpose(hi);
     uint8_t *row = out_ptrs ? out_ptrs[r] : out_base + s * out_stripe + r * out_row;
-    const uint64_t col = g * 32, remain = N - col;
+    const uint64_t col = (g0 + g) * 32, remain = N - col;
     store32(row + col, remain, lo);
     store32(row + N + col, remain, hi);
+  }
+}
+
+// Glue of the interpolation of k points that are not a power of two (src/fft.rs:198-239):
+// dst[dst_start + i] ^= c * src[src_start + i] for i < count, per stripe; with
+// cols == nullptr the constant is 1 (plain XOR).
+__global__ void __launch_bounds__(kFft16Threads)
+    fft16_mulxor_kernel(const uint32_t *src, uint32_t src_regs, uint32_t src_start, uint32_t *dst, uint32_t dst_regs,
+                        uint32_t dst_start, uint32_t count, uint64_t G, uint32_t n_stripes, const uint16_t *cols) {
+  __shared__ __align__(16) uint32_t mk[256];
+  if (cols) {
+    for (uint32_t t = threadIdx.x; t < 256; t += blockDim.x) mk[t] = ((cols[t & 15] >> (t >> 4)) & 1) ? ~0u : 0u;
+    __syncthreads();
+  }
+  const uint64_t total = (uint64_t)n_stripes * count * G;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t g = t % G, si = t / G;
+    const uint64_t i = si % count, s = si / count;
+    Reg16 x, y;
+    load_reg16(src + ((s * src_regs + src_start + i) * G + g) * 16, x);
+    uint32_t *d = dst + ((s * dst_regs + dst_start + i) * G + g) * 16;
+    load_reg16(d, y);
+    if (cols)
+      mul16_acc(y, x, mk);
+    else
+      xor16(y, x);
+    store_reg16(d, y);
   }
 }
 

@@ -11,7 +11,7 @@
 
 #include "runtime.hpp"
 #include "gf_host.hpp"
-#include "kernels_fft16.cuh"
+#include "fft16.hpp"
 #include "kernels_lagrange.cuh"
 #include "kernels_matrix.cuh"
 
@@ -28,10 +28,8 @@ struct Gen16 {
   int device = 0;
   size_t k = 0, m = 0;
   uint32_t *d_split = nullptr;
-  // FFT route (k a power of two >= 2): per transform (the interpolation with beta 0,
-  // then one forward transform per coset cK of parity points) k - 1 constants, each as
-  // its 16 columns c * 2^p.
-  uint32_t fft_cosets = 0;
+  // FFT route (any k >= 2): the step program and its constants on the device.
+  std::unique_ptr<Fft16Program> fft;
   uint16_t *d_fft_cols = nullptr;
   ~Gen16() {
     cudaSetDevice(device);
@@ -40,152 +38,25 @@ struct Gen16 {
   }
 };
 
-// WHAT[l][x] of the tower field: W_0(x) = x, W_{j+1}(x) = W_j(x) (W_j(x) + W_j(2^j)),
-// each level scaled so that W_l(2^l) = 1 (src/fft16.rs:42-70). Evaluated per point by
-// running the recurrence, which needs the unscaled pivots W_j(2^j).
-struct What16 {
-  uint16_t pivot[16], pivot_inv[16];
-  What16() {
-    for (int l = 0; l < 16; l++) {
-      pivot[l] = raw(l, (uint16_t)(1u << l));
-      pivot_inv[l] = gf16_inv(pivot[l]);
-    }
-  }
-  uint16_t raw(int l, uint16_t x) const {
-    uint16_t w = x;
-    for (int j = 0; j < l; j++) w = gf16_mul(w, (uint16_t)(w ^ pivot[j]));
-    return w;
-  }
-  uint16_t operator()(int l, uint16_t x) const { return gf16_mul(raw(l, x), pivot_inv[l]); }
-};
-
-static bool is_pow2(size_t x) { return x && !(x & (x - 1)); }
-
-static int log2_exact(size_t x) {
-  int l = 0;
-  while (((size_t)1 << l) < x) l++;
-  return l;
-}
-
-// Constants of every transform of the FFT route, as 16 columns each, onto the device.
-static int build_fft16_plan(Gen16 &g) {
-  const size_t K = g.k;
-  if (!is_pow2(K) || K < 2) return RS_OK;
-  const int lg = log2_exact(K);
-  const uint32_t cosets = (uint32_t)((g.m + K - 1) / K);
-  static const What16 what;
-  std::vector<uint16_t> cols((size_t)(1 + cosets) * (K - 1) * 16);
-  for (uint32_t t = 0; t <= cosets; t++) {
-    const size_t beta = (size_t)t * K;
-    for (int l = 0; l < lg; l++) {
-      for (size_t j = 0; j < (K >> (l + 1)); j++) {
-        const size_t base = j << (l + 1);
-        const uint16_t c = what(l, (uint16_t)(beta ^ base));
-        uint16_t *col = &cols[((size_t)t * (K - 1) + (K - (K >> l)) + j) * 16];
-        for (int p = 0; p < 16; p++) col[p] = gf16_mul(c, (uint16_t)(1u << p));
-      }
-    }
-  }
-  RSB_CU(cudaMalloc(&g.d_fft_cols, cols.size() * 2));
-  RSB_CU(cudaMemcpy(g.d_fft_cols, cols.data(), cols.size() * 2, cudaMemcpyHostToDevice));
-  g.fft_cosets = cosets;
+static int build_fft16(Gen16 &g) {
+  auto p = std::make_unique<Fft16Program>();
+  if (!fft16_build(g.k, g.m, *p)) return RS_OK;
+  RSB_CU(cudaMalloc(&g.d_fft_cols, p->cols.size() * 2));
+  RSB_CU(cudaMemcpy(g.d_fft_cols, p->cols.data(), p->cols.size() * 2, cudaMemcpyHostToDevice));
+  g.fft = std::move(p);
   return RS_OK;
 }
 
-// Estimated per-symbol work of the two routes (LOP3 per 32 symbols): the matrix kernel
-// spends about 26 per coefficient, a butterfly about 290 (256 masked XORs plus adds);
-// passes also move the scratch through L2, counted as twice their arithmetic.
-static bool fft16_preferred(const Gen16 &g) {
-  if (!g.d_fft_cols) return false;
-  const double lg = log2_exact(g.k);
-  const double fft = 2.0 * (1 + g.fft_cosets) * (g.k / 2.0) * lg * 290.0;
-  const double matrix = (double)g.k * g.m * 26.0 * 32.0 / 4.0;
-  return fft < matrix;
-}
-
-// Encode on the FFT route: stripes s of k data rows (in_base + s*in_stripe + r*in_row)
-// to m parity rows (out_base + s*out_stripe + j*out_row); with d_ptrs (one stripe) the
-// rows are the k + m device pointers of that table instead. Scratch is stream-ordered
-// and sized so a wave of stripes stays within 64 MiB.
+// FFT-route encode with stream-ordered scratch of at most 256 MiB.
 static int fft16_encode(const Gen16 &g, const uint8_t *in_base, uint64_t in_row, uint64_t in_stripe,
                         uint8_t *out_base, uint64_t out_row, uint64_t out_stripe, size_t n_stripes, size_t len,
                         uint8_t *const *d_ptrs, cudaStream_t st) {
-  const uint32_t K = (uint32_t)g.k;
-  const int lg = log2_exact(K);
-  const uint64_t N = len / 2, G = (N + 31) / 32;
-  const uint32_t cosets = g.fft_cosets;
-  const uint64_t reg_words = G * 16, buf_words = (uint64_t)K * reg_words;
-  const uint64_t per_stripe = buf_words * 4 * (cosets > 1 ? 2 : 1);
-  const size_t wave = (size_t)std::max<uint64_t>(1, std::min<uint64_t>(n_stripes, (64ull << 20) / per_stripe));
-  uint32_t *scratch = nullptr;
-  RSB_CU(cudaMallocAsync(&scratch, wave * per_stripe, st));
-  int rc = RS_OK;
-  auto pass = [&](const uint32_t *src, uint32_t *dst, const uint16_t *cols, int level, int lv, bool inverse,
-                  uint32_t stripes) -> int {
-    Fft16PassArgs a{};
-    a.src = src;
-    a.dst = dst;
-    a.cols = cols;
-    a.R = K;
-    a.level = (uint32_t)level;
-    a.G = G;
-    a.n_stripes = stripes;
-    a.inverse = inverse;
-    const uint64_t tasks = (uint64_t)stripes * ((G + 31) / 32);
-    const unsigned threads = (unsigned)(32 * std::min<uint64_t>(8, tasks));
-    const unsigned gy = (unsigned)std::min<uint64_t>(65535, (tasks * 32 + threads - 1) / threads);
-    if (lv == 2)
-      fft16_pass_kernel<2><<<dim3(K / 4, gy), threads, 0, st>>>(a);
-    else
-      fft16_pass_kernel<1><<<dim3(K / 2, gy), threads, 0, st>>>(a);
-    g_launches++;
-    RSB_CU(cudaGetLastError());
-    return RS_OK;
-  };
-  auto copy_grid = [&](uint64_t items) {
-    return (unsigned)std::min<uint64_t>((items + kFft16Threads - 1) / kFft16Threads, 148ull * 16);
-  };
-  for (size_t s0 = 0; s0 < n_stripes && rc == RS_OK; s0 += wave) {
-    const uint32_t ns = (uint32_t)std::min(wave, n_stripes - s0);
-    uint32_t *C = scratch, *W = cosets > 1 ? scratch + wave * buf_words : scratch;
-    fft16_load_kernel<<<copy_grid((uint64_t)ns * K * G), kFft16Threads, 0, st>>>(
-        in_base + s0 * in_stripe, in_row, in_stripe, reinterpret_cast<const uint8_t *const *>(d_ptrs), K, N, G, ns,
-        K, C);
-    g_launches++;
-    if (cudaGetLastError() != cudaSuccess) {
-      rc = RS_ERR_CUDA;
-      break;
-    }
-    // Interpolation: levels 0 .. lg-1 in pairs, an odd top level alone.
-    int L = 0;
-    for (; L + 1 < lg && rc == RS_OK; L += 2) rc = pass(C, C, g.d_fft_cols, L, 2, true, ns);
-    if (L < lg && rc == RS_OK) rc = pass(C, C, g.d_fft_cols, L, 1, true, ns);
-    for (uint32_t c = 1; c <= cosets && rc == RS_OK; c++) {
-      const uint16_t *cols = g.d_fft_cols + (size_t)c * (K - 1) * 16;
-      const uint32_t *src = C;
-      // Evaluation on coset cK: levels lg-1 .. 0, an odd top level first.
-      int top = lg - 1;
-      if (lg % 2 == 1) {
-        rc = pass(src, W, cols, top, 1, false, ns);
-        src = W;
-        top--;
-      }
-      for (int l = top - 1; l >= 0 && rc == RS_OK; l -= 2) {
-        rc = pass(src, W, cols, l, 2, false, ns);
-        src = W;
-      }
-      if (rc) break;
-      const uint32_t rows = (uint32_t)std::min<uint64_t>(K, g.m - (uint64_t)(c - 1) * K);
-      fft16_store_kernel<<<copy_grid((uint64_t)ns * rows * G), kFft16Threads, 0, st>>>(
-          W, K, rows, N, G, ns,
-          d_ptrs ? nullptr : out_base + s0 * out_stripe + (uint64_t)(c - 1) * K * out_row, out_row, out_stripe,
-          d_ptrs ? d_ptrs + K + (size_t)(c - 1) * K : nullptr);
-      g_launches++;
-      if (cudaGetLastError() != cudaSuccess) rc = RS_ERR_CUDA;
-    }
-  }
+  const size_t bytes = fft16_scratch_bytes(*g.fft, n_stripes, len, (size_t)256 << 20);
+  uint8_t *scratch = nullptr;
+  RSB_CU(cudaMallocAsync(&scratch, bytes, st));
+  int rc = fft16_run(*g.fft, g.d_fft_cols, scratch, bytes, in_base, in_row, in_stripe, out_base, out_row, out_stripe,
+                     d_ptrs, n_stripes, len, st);
   cudaFreeAsync(scratch, st);
-  if (rc == RS_ERR_CUDA) set_cuda_error(cudaGetLastError(), "fft16 encode launch");
   return rc;
 }
 
@@ -259,8 +130,8 @@ struct rs16_codec {
 namespace rsb {
 static bool use_fft16(const rs16_codec *c) {
   int r = c->route.load();
-  if (r == 1 || !c->gen->d_fft_cols) return false;
-  return r == 2 || fft16_preferred(*c->gen);
+  if (r == 1 || !c->gen->fft) return false;
+  return r == 2 || fft16_preferred(*c->gen->fft);
 }
 }  // namespace rsb
 
@@ -400,7 +271,7 @@ int rs16_new(size_t k, size_t m, rs16_t **out) {
   int st0 = lagrange16_device(nodes, targets, &d);
   gen->d_split = d;
   if (st0) return st0;
-  RSB_TRY(build_fft16_plan(*gen));
+  RSB_TRY(build_fft16(*gen));
   auto c = new (std::nothrow) rs16_codec();
   if (!c) return RS_ERR_ALLOC;
   c->gen = gen;

@@ -1,7 +1,8 @@
 """FFT route of ReedSolomon16: the bitsliced tower LCH transform (src/fft16.rs) must give
-the bytes of the symbol-wise oracle and of the matrix route, for every power-of-two k,
-parity counts below, at and across multiples of k (several cosets), and shard lengths
-that are not multiples of the 32-symbol groups.
+the bytes of the symbol-wise oracle and of the matrix route, for power-of-two k and for
+k between powers of two (the recursive interpolation of src/fft.rs:198-239), parity
+counts below, at and across multiples of the transform size (several cosets), and shard
+lengths that are not multiples of the 32-symbol groups.
 """
 import numpy as np
 import pytest
@@ -20,7 +21,7 @@ def _encode(rs, data, m):
     return np.array(shards[k:])
 
 
-@pytest.mark.parametrize("k", [2, 4, 8, 16, 32, 64, 128, 256])
+@pytest.mark.parametrize("k", [2, 3, 4, 5, 6, 7, 8, 11, 16, 17, 24, 32, 33, 63, 64, 100, 128, 200, 256, 300])
 def test_fft_route_matches_oracle(gpu, O, k):
     for m in sorted({1, max(1, k // 2), k, k + 1, 2 * k, 3 * k - 1}):
         rs = gpu.ReedSolomon16(k, m)
@@ -86,7 +87,26 @@ def test_fft_route_device_pointer_table(gpu, O):
     assert np.array_equal(got, O.encode16(k, m, data))
 
 
+def test_fft_route_large_odd_k(gpu):
+    import torch
+
+    for k, m in [(1000, 3000), (2500, 700), (129, 12000)]:
+        S = 1026
+        rs = gpu.ReedSolomon16(k, m)
+        assert rs.encode_route() == "fft"
+        g = torch.Generator(device="cuda").manual_seed(k)
+        d = torch.randint(0, 256, (2, k, S), dtype=torch.uint8, device="cuda", generator=g)
+        p_fft = torch.empty((2, m, S), dtype=torch.uint8, device="cuda")
+        p_mat = torch.empty_like(p_fft)
+        rs.encode_batch_dev(d, p_fft, S, 2)
+        rs.set_route("matrix")
+        rs.encode_batch_dev(d, p_mat, S, 2)
+        torch.cuda.synchronize()
+        assert torch.equal(p_fft, p_mat), (k, m)
+
+
 def test_route_choice(gpu):
-    assert gpu.ReedSolomon16(3, 2).encode_route() == "matrix"  # k not a power of two
-    assert gpu.ReedSolomon16(2, 1).encode_route() == "matrix"  # too small to pay off
+    assert gpu.ReedSolomon16(3, 2).encode_route() == "matrix"  # too small to pay off
+    assert gpu.ReedSolomon16(2, 1).encode_route() == "matrix"
     assert gpu.ReedSolomon16(256, 256).encode_route() == "fft"
+    assert gpu.ReedSolomon16(300, 500).encode_route() == "fft"
