@@ -20,6 +20,8 @@ Other workloads (one JSON line each, 1 GPU, no reference arm):
                          (graph) against one plain launch per stripe
     --workload rs16      ReedSolomon16 (1024,1024) and (4096,12288), 2 KiB shards
     --workload serve     Poisson request stream at 50k req/s through the request server
+    --workload tuner     exhaustive autotuning of sampled workloads, the MLP cost model
+                         trained on them, held-out regret (model and default)
 """
 import argparse
 import json
@@ -48,7 +50,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--stripes", type=int, default=1024, help="stripes per step per GPU")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--workload", default="encode", choices=["encode", "stripes", "mixed", "rs16", "serve"])
+    ap.add_argument("--workload", default="encode",
+                    choices=["encode", "stripes", "mixed", "rs16", "serve", "tuner"])
+    ap.add_argument("--tuner-workloads", type=int, default=10000,
+                    help="workloads the tuner times (about 5 applicable configurations each)")
     ap.add_argument("--requests", type=int, default=400, help="requests of the serve workload")
     return ap.parse_args()
 
@@ -315,6 +320,10 @@ def run_workload(args):
         elif args.workload == "rs16":
             res = workloads.rs16_shapes()
             line = {"metric": "ReedSolomon16 encode/reconstruct GB/s", "unit": "GB/s", "results": res}
+        elif args.workload == "tuner":
+            res = workloads.tuner_regret(n_workloads=args.tuner_workloads)
+            line = {"metric": "cost-model route/tile regret vs exhaustive tuning (held out)", "unit": "fraction",
+                    "value": res["regret_model"], "higher_is_better": False, "results": res}
         else:
             res = workloads.serve_poisson(count=args.requests)
             line = {"metric": "request server p50/p99 latency and GB/s, Poisson 50k req/s", "unit": "GB/s",

@@ -19,6 +19,10 @@
 
 namespace rsb {
 
+// Scratch budget per run: a wave of registers this size stays resident in L2 across
+// the passes (the B200's L2 is 126 MB).
+constexpr size_t kFft16ScratchBudget = (size_t)48 << 20;
+
 struct Fft16Step {
   enum Kind : uint8_t { kTransform, kMulXor } kind;
   uint8_t src_buf, dst_buf;  // 0 = C, 1 = S, 2 = W

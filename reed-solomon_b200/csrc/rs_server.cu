@@ -36,6 +36,7 @@
 #include <vector>
 
 #include "codec8.hpp"
+#include "fft16.hpp"
 #include "gf_host.hpp"
 #include "kernels_batch.cuh"
 #include "kernels_fft.cuh"
@@ -112,6 +113,8 @@ struct Table {
   uint64_t last_use = 0;
   cudaEvent_t ready = nullptr;
   bool stale = false;  // its build failed: never reused, dropped once idle
+  // GF(2^16) encode on the FFT route: the program; the span then holds its constants.
+  std::shared_ptr<const Fft16Program> fft16;
 };
 
 static uint64_t table_key(int field, size_t k, size_t m) {
@@ -119,6 +122,8 @@ static uint64_t table_key(int field, size_t k, size_t m) {
 }
 
 static size_t table_bytes(int field, size_t k, size_t m) { return field == 8 ? k * m : k * m * 4; }
+
+static size_t fft16_table_bytes(const Fft16Program &p) { return p.cols.size() * 2; }
 
 struct Req {
   rs_request r{};
@@ -133,6 +138,9 @@ struct Req {
   Table *table = nullptr;
   bool builds_table = false;
   size_t table_host_off = 0;  // GF(2^8) rows to upload, inside the pinned image
+  std::shared_ptr<const Fft16Program> fft16;      // GF(2^16) encode on the FFT route
+  std::shared_ptr<const Fft16Program> candidate;  // its program, built at submit
+  size_t scratch_budget = 0;                       // FFT scratch limit
 };
 
 struct Group;
@@ -207,7 +215,10 @@ static void size_request(Req &q, bool new_table) {
     }
     if (new_table) up += up256(k * m);  // generator rows staged for upload
   } else {
-    if (r.op == RS_BATCH_ENCODE) {
+    if (r.op == RS_BATCH_ENCODE && q.fft16) {
+      if (new_table) up += up256(fft16_table_bytes(*q.fft16));  // constants staged for upload
+      dev += up256(fft16_scratch_bytes(*q.fft16, 1, r.row_len, q.scratch_budget));
+    } else if (r.op == RS_BATCH_ENCODE) {
       if (new_table) {
         up += up256(k * 2) + up256(m * 2);                 // nodes | targets
         dev += up256(k * 2) + up256(m * 2) + up256(m * 4);  // w | ell | hit
@@ -276,8 +287,25 @@ static bool reserve(rs_server *s, Req &q) {
   if (it != s->tables.end() && it->second->stale) return false;
   bool need_table = r.field == 8 || r.op == RS_BATCH_ENCODE;
   bool new_table = need_table && it == s->tables.end();
+  q.fft16.reset();
+  q.scratch_budget = std::min<size_t>(kFft16ScratchBudget, s->cfg.arena_bytes / 8);
+  if (r.field == 16 && r.op == RS_BATCH_ENCODE) {
+    if (!new_table) {
+      q.fft16 = it->second->fft16;
+    } else {
+      q.fft16 = q.candidate;
+      // The FFT route must fit the arena on its own; otherwise the matrix route.
+      if (q.fft16) {
+        size_request(q, true);
+        if (up256(q.up_bytes) + up256(q.dev_bytes) + up256(fft16_table_bytes(*q.fft16)) > s->cfg.arena_bytes)
+          q.fft16.reset();
+      }
+    }
+  }
   size_request(q, new_table);
-  size_t tb = new_table ? table_bytes(r.field, r.data_shards, r.parity_shards) : 0;
+  size_t tb = !new_table ? 0
+              : q.fft16 ? fft16_table_bytes(*q.fft16)
+                        : table_bytes(r.field, r.data_shards, r.parity_shards);
   size_t total = up256(payload_bytes(r)) + up256(q.up_bytes) + up256(q.dev_bytes) + up256(tb);
   if (!evict_for(s, total)) return false;
   Span pay, up, dev, host, tab;
@@ -303,6 +331,7 @@ static bool reserve(rs_server *s, Req &q) {
       t->k = r.data_shards;
       t->m = r.parity_shards;
       t->span = tab;
+      t->fft16 = q.fft16;
       it = s->tables.emplace(key, std::move(t)).first;
       q.builds_table = true;
       s->st.table_builds++;
@@ -555,6 +584,20 @@ static int enqueue_gf16(rs_server *s, Group &g, cudaStream_t st) {
   a.n_sym = r.row_len / 2;
   a.n_stripes = 1;
   a.k = (uint32_t)k;
+  if (r.op == RS_BATCH_ENCODE && q.fft16) {
+    const Fft16Program &p = *q.fft16;
+    if (q.builds_table) {
+      memcpy(h, p.cols.data(), fft16_table_bytes(p));
+      RSB_CU(cudaMemcpyAsync(s->arena + q.table->span.off, h, fft16_table_bytes(p), cudaMemcpyHostToDevice, st));
+      RSB_TRY(mark_table(q, st));
+    }
+    RSB_TRY(wait_table(q, st));
+    const uint64_t before = g_launches.load();
+    RSB_TRY(fft16_run(p, reinterpret_cast<const uint16_t *>(s->arena + q.table->span.off), d, q.dev.bytes, rows,
+                      r.row_len, 0, rows + k * r.row_len, r.row_len, 0, nullptr, 1, r.row_len, st));
+    g.launches += g_launches.load() - before;
+    return stage_out(s, q, st);
+  }
   if (r.op == RS_BATCH_ENCODE) {
     if (q.builds_table) {
       uint16_t *nodes = reinterpret_cast<uint16_t *>(h), *tg = reinterpret_cast<uint16_t *>(h + up256(k * 2));
@@ -840,13 +883,28 @@ int rs_server_submit(rs_server_t *s, const rs_request *reqs, size_t n, int *stat
     q->submit_ns = t;
     int st = validate(reqs[i], *q);
     if (st == RS_OK) {
-      // Largest working set it could ever need: it must fit an empty arena.
+      // Largest working set it could ever need (building its table) must fit an empty
+      // arena on at least one route.
+      const rs_request &r = reqs[i];
       size_request(*q, true);
-      size_t tb = (reqs[i].field == 8 || reqs[i].op == RS_BATCH_ENCODE)
-                      ? table_bytes(reqs[i].field, reqs[i].data_shards, reqs[i].parity_shards)
-                      : 0;
-      size_t need = up256(payload_bytes(reqs[i])) + up256(q->up_bytes) + up256(q->dev_bytes) + up256(tb);
-      if (need > s->cfg.arena_bytes || up256(q->up_bytes) > s->cfg.pinned_bytes) st = RS_ERR_TOO_LARGE;
+      size_t tb = (r.field == 8 || r.op == RS_BATCH_ENCODE) ? table_bytes(r.field, r.data_shards, r.parity_shards)
+                                                             : 0;
+      size_t need = up256(payload_bytes(r)) + up256(q->up_bytes) + up256(q->dev_bytes) + up256(tb);
+      bool fits = need <= s->cfg.arena_bytes && up256(q->up_bytes) <= s->cfg.pinned_bytes;
+      if (r.field == 16 && r.op == RS_BATCH_ENCODE) {
+        auto p = std::make_shared<Fft16Program>();
+        if (fft16_build(r.data_shards, r.parity_shards, *p) && fft16_preferred(*p)) {
+          q->candidate = p;
+          q->fft16 = p;
+          q->scratch_budget = std::min<size_t>(kFft16ScratchBudget, s->cfg.arena_bytes / 8);
+          size_request(*q, true);
+          size_t need_fft = up256(payload_bytes(r)) + up256(q->up_bytes) + up256(q->dev_bytes) +
+                            up256(fft16_table_bytes(*p));
+          fits = fits || (need_fft <= s->cfg.arena_bytes && up256(q->up_bytes) <= s->cfg.pinned_bytes);
+          q->fft16.reset();
+        }
+      }
+      if (!fits) st = RS_ERR_TOO_LARGE;
     }
     if (statuses) statuses[i] = st;
     if (st != RS_OK) {

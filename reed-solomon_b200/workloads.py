@@ -182,6 +182,10 @@ def rs16_shapes(shapes=((1024, 1024, 64), (4096, 12288, 2)), S=2048, seed=4, rep
             rs.encode_batch_dev(rows, rows[:, k:], S, stripes, data_stride=stride, parity_stride=stride)
 
         t_enc = _time(enc, reps)
+        route = rs.encode_route()
+        rs.set_route("matrix")
+        t_mat = _time(enc, 1)
+        rs.set_route("auto")
         full = rows[0].clone()
         present = np.ones(n, np.uint8)
         present[rng.choice(n, size=m, replace=False)] = 0  # m erasures at random positions
@@ -193,13 +197,44 @@ def rs16_shapes(shapes=((1024, 1024, 64), (4096, 12288, 2)), S=2048, seed=4, rep
 
         t_rec = _time(rec, 1, warmup=0)
         exact = bool(torch.equal(rows[0], full))
-        out.append({"k": k, "m": m, "shard_bytes": S, "stripes": stripes, "route": rs.encode_route(),
+        out.append({"k": k, "m": m, "shard_bytes": S, "stripes": stripes, "route": route,
                     "encode_gbs": stripes * n * S / t_enc / 1e9, "encode_ms_per_stripe": t_enc / stripes * 1e3,
+                    "encode_matrix_gbs": stripes * n * S / t_mat / 1e9,
                     "reconstruct_m_erasures_gbs": (k + m) * S / t_rec / 1e9,
                     "reconstruct_ms": t_rec * 1e3, "reconstruct_bit_exact": exact})
         del rows
         torch.cuda.empty_cache()
     return out
+
+
+# ---- autotuner and learned cost model ----
+
+def tuner_regret(n_workloads=1500, seed=11, train_frac=0.8, max_bytes=32 << 20, epochs=300):
+    """Exhaustive tuning of sampled GF(2^8) workloads (every applicable route / tile,
+    timed on the GPU), the FP32 MLP cost model trained on most of them by the library's
+    CUDA kernels, and its regret on the held-out rest against exhaustive tuning, beside
+    the regret of the default choice (the method without the model)."""
+    from . import tuner
+
+    t0 = time.perf_counter()
+    work = tuner.sample_workloads(n_workloads, seed=seed, max_bytes=max_bytes)
+    X, T = tuner.collect(work, reps=2)
+    collect_s = time.perf_counter() - t0
+    n_tr = int(len(work) * train_frac)
+    m = tuner.CostModel(hidden=64, seed=seed)
+    t1 = time.perf_counter()
+    hist = m.fit(X[:n_tr], T[:n_tr], epochs=epochs, lr=3e-3, batch=256)
+    train_s = time.perf_counter() - t1
+    te = slice(n_tr, len(work))
+    choice = m.choose(X[te], T[te])
+    default = tuner.default_choice(work[te], T[te])
+    best = np.nanargmin(T[te], axis=1)
+    return {"workloads": len(work), "timings": int(np.isfinite(T).sum()), "train": n_tr,
+            "held_out": len(work) - n_tr, "collect_s": collect_s, "train_s": train_s,
+            "final_loss": hist[-1], "regret_model": tuner.regret(T[te], choice),
+            "regret_default": tuner.regret(T[te], default),
+            "model_picks_best": float(np.mean(choice == best)),
+            "default_picks_best": float(np.mean(default == best))}
 
 
 # ---- serving: Poisson request stream through the request server ----

@@ -167,9 +167,12 @@ def test_resident_tables_hit_and_evict(gpu, O):
         assert np.array_equal(_result(req), expect)
     s = srv.stats()
     assert s["table_builds"] == 1 and s["table_hits"] == 5
-    # Shapes whose tables (m*k*4 bytes) cannot all stay resident force evictions.
-    for i, (k, m) in enumerate([(500, 400), (400, 500), (450, 450), (500, 400)]):
-        req, expect = _make(O, (16, ENC, k, m, 64, False), seed=950 + i)
+    srv.close()
+    # Matrix-route shapes (few parity rows) whose generators (m*k*4 bytes, 32 KB each)
+    # cannot all stay resident in a 256 KiB arena force evictions.
+    srv = gpu.Server(arena_bytes=256 << 10, slots=8)
+    for i in range(12):
+        req, expect = _make(O, (16, ENC, 400 + i, 20, 64, False), seed=950 + i)
         req["tag"] = 100 + i
         srv.submit([req])
         srv.wait(1)
