@@ -291,7 +291,7 @@ def run_ours(args, rank, world):
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
-        if world == 1:
+        if world == 1 and args.cpu_seconds > 0:  # 0 skips it (profiling runs)
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         print(json.dumps(line), flush=True)
 

@@ -105,6 +105,7 @@ void interpolate(Fft16Program &p, uint32_t start, uint32_t n, uint32_t beta, uin
   if (half > 1) {
     transform(p, 0, start, 1, 0, half, beta ^ half, false);
     mulxor(p, 1, 0, start + half, k - half, 1);
+    p.uses_s = true;
   } else {
     mulxor(p, 0, start, start + half, k - half, 1);
   }
@@ -135,6 +136,7 @@ bool fft16_build(size_t k, size_t m, Fft16Program &p) {
     e.parity_row = lo - k;
     p.evals.push_back(e);
   }
+  p.eval_in_place = p.evals.size() == 1;
   return true;
 }
 
@@ -167,7 +169,7 @@ int fft16_run(const Fft16Program &p, const uint16_t *d_cols, uint8_t *scratch, s
     wave = 1;
     gc = scratch_bytes / per_group;
   }
-  const uint32_t regs_of[3] = {t, std::max<uint32_t>(1, t / 2), t};
+  const uint32_t regs_of[3] = {t, p.regs_s(), p.eval_in_place ? t : p.regs_w()};
   auto grid_for = [](uint64_t items) {
     return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((items + kFft16Threads - 1) / kFft16Threads, 148 * 16));
   };
@@ -178,7 +180,7 @@ int fft16_run(const Fft16Program &p, const uint16_t *d_cols, uint8_t *scratch, s
       uint32_t *buf[3];
       buf[0] = reinterpret_cast<uint32_t *>(scratch);
       buf[1] = buf[0] + (uint64_t)ns * regs_of[0] * gn * 16;
-      buf[2] = buf[1] + (uint64_t)ns * regs_of[1] * gn * 16;
+      buf[2] = p.eval_in_place ? buf[0] : buf[1] + (uint64_t)ns * regs_of[1] * gn * 16;
       auto pass = [&](const Fft16Step &s, const uint32_t *src, uint32_t src_regs, uint32_t src_start, int level,
                       int lv) -> int {
         Fft16PassArgs a{};

@@ -47,7 +47,11 @@ struct Fft16Program {
   std::vector<Fft16Eval> evals;
   std::vector<uint16_t> cols;  // 16 columns c * 2^p per constant
   uint64_t butterflies = 0;    // per 32-symbol group (route estimate)
-  uint32_t regs() const { return t + t / 2 + t; }  // C + S + W per stripe and group
+  bool uses_s = false;         // the interpolation needs S (k not a power of two)
+  bool eval_in_place = false;  // a single evaluation runs on C itself (no W)
+  uint32_t regs_s() const { return uses_s ? t / 2 : 0; }
+  uint32_t regs_w() const { return eval_in_place ? 0 : t; }
+  uint32_t regs() const { return t + regs_s() + regs_w(); }  // per stripe and group
 };
 
 // False (no FFT route) for k < 2.

@@ -337,6 +337,8 @@ struct FftArgs {
   const FftItem *items;
   uint32_t n_items;
   uint64_t total_groups;
+  // Pointer-table form: every shard pointer is 16-byte aligned (set by the host).
+  int ptrs_aligned;
 };
 
 // Where one lane pair's 32-column group lives.
@@ -410,18 +412,30 @@ __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// Byte paths for the last, partial group of a shard or unaligned rows, kept out of
+// line: the unrolled per-shard code then holds a call instead of a byte loop, so these
+// rarely taken fallbacks do not fill the instruction cache.
+static __device__ __noinline__ void stage32_bytes(uint8_t *slot, int half, const uint8_t *p, uint64_t remain) {
+  uint32_t w[8];
+  load32(p, remain, w);
+  *reinterpret_cast<uint4 *>(slot) = make_uint4(w[0], w[1], w[2], w[3]);
+  *reinterpret_cast<uint4 *>(slot + half) = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+static __device__ __noinline__ void store32_bytes(uint8_t *p, uint64_t remain, uint4 lo, uint4 hi) {
+  const uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+  store32(p, remain, w);
+}
+
 // Stage the 32 bytes at p (remain of them valid) into this thread's slot: two async
-// 16-byte copies when aligned and whole, else a zero-filled byte path.
+// 16-byte copies when aligned and whole, else the zero-filled byte path.
 template <int HALF>
 __device__ __forceinline__ void stage32(uint8_t *slot, const uint8_t *p, uint64_t remain) {
   if (remain >= 32 && (((uintptr_t)p & 15u) == 0)) {
     cp_async16(slot, p);
     cp_async16(slot + HALF, p + 16);
   } else {
-    uint32_t w[8];
-    load32(p, remain, w);
-    *reinterpret_cast<uint4 *>(slot) = make_uint4(w[0], w[1], w[2], w[3]);
-    *reinterpret_cast<uint4 *>(slot + HALF) = make_uint4(w[4], w[5], w[6], w[7]);
+    stage32_bytes(slot, HALF, p, remain);
   }
 }
 
@@ -454,10 +468,29 @@ __global__ void __launch_bounds__(THREADS, CTAS)
     else
       return l.in0 + (uint64_t)((j << W) | q) * l.in_rs;
   };
+  // Whole 32-byte groups on 16-byte aligned rows (every group but a shard's last, for
+  // aligned stripes) take the unrolled fast paths; the decision is made once per round.
+  auto whole = [&](const FftLoc &l) -> bool {
+    if constexpr (PTRS)
+      return l.remain >= 32 && a.ptrs_aligned;
+    else
+      return l.remain >= 32 &&
+             ((reinterpret_cast<uintptr_t>(l.in0) | reinterpret_cast<uintptr_t>(l.out0) | l.in_rs | l.out_rs) &
+              15u) == 0;
+  };
   auto prefetch = [&](uint64_t grp) {
     const FftLoc l = fft_locate(a, grp);
+    if (whole(l)) {
 #pragma unroll
-    for (int j = 0; j < S; j++) stage32<St::kHalf>(mine + j * St::kSlot, in_ptr(l, j) + l.col, l.remain);
+      for (int j = 0; j < S; j++) {
+        const uint8_t *p = in_ptr(l, j) + l.col;
+        cp_async16(mine + j * St::kSlot, p);
+        cp_async16(mine + j * St::kSlot + St::kHalf, p + 16);
+      }
+    } else {
+#pragma unroll 1
+      for (int j = 0; j < S; j++) stage32<St::kHalf>(mine + j * St::kSlot, in_ptr(l, j) + l.col, l.remain);
+    }
     cp_async_commit();
   };
 
@@ -496,6 +529,7 @@ __global__ void __launch_bounds__(THREADS, CTAS)
     // Evaluate on coset K: forward transform, levels LG-1 .. 0.
     levels_down<K, W, LG - 1, K, SYNC>(r, q, qm);
     if (live) {
+      const bool fast = whole(loc);
 #pragma unroll
       for (int j = 0; j < S; j++) {
         uint8_t *row;
@@ -507,7 +541,13 @@ __global__ void __launch_bounds__(THREADS, CTAS)
 #pragma unroll
         for (int b = 0; b < 8; b++) w[b] = r[j][b];
         bit_transpose(w);
-        store32(row + col, remain, w);
+        const uint4 lo = make_uint4(w[0], w[1], w[2], w[3]), hi = make_uint4(w[4], w[5], w[6], w[7]);
+        if (fast) {
+          *reinterpret_cast<uint4 *>(row + col) = lo;
+          *reinterpret_cast<uint4 *>(row + col + 16) = hi;
+        } else {
+          store32_bytes(row + col, remain, lo, hi);
+        }
       }
     }
     phase_sync<SYNC>();
@@ -691,8 +731,11 @@ inline int launch_fft8_ptrs(const FftShape &sh, uint8_t *const *shards, uint64_t
   a.n_stripes = 1;
   a.groups_per_stripe = (uint32_t)((len + 31) / 32);
   PtrTableT<true> pt;
+  uintptr_t bits = 0;
   for (int i = 0; i < sh.k; i++) pt.in[i] = shards[i];
   for (int j = 0; j < sh.m; j++) pt.out[j] = shards[sh.k + j];
+  for (int i = 0; i < sh.k + sh.m; i++) bits |= reinterpret_cast<uintptr_t>(shards[i]);
+  a.ptrs_aligned = (bits & 15u) == 0;
   return launch_fft_any<true>(sh, a, pt, st);
 }
 

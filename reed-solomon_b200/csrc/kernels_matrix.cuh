@@ -266,7 +266,22 @@ struct Apply16Args {
   uint64_t n_sym;  // symbols per shard (shard bytes / 2)
   uint32_t n_stripes;
   uint32_t *mismatch;
+  uint32_t row_chunk;  // output rows per CTA (grid.z), set by gf16_launch_shape
 };
+
+// Launch shape of gf16_matrix_kernel: CTAs as wide as the shard needs (8 symbols per
+// thread, 32..256 threads), and output-row chunks halved from 64 down to 4 until the
+// grid has two CTAs per SM, so single stripes of short shards still fill the GPU.
+inline void gf16_launch_shape(Apply16Args &a, int sms, dim3 &grid, unsigned &threads) {
+  const uint64_t need = (a.n_sym + 7) / 8;
+  threads = (unsigned)std::min<uint64_t>(kThreads, std::max<uint64_t>(32, (need + 31) / 32 * 32));
+  const uint64_t tiles = (a.n_sym + threads * 8ull - 1) / (threads * 8ull);
+  const uint32_t stripes = std::min<uint32_t>(a.n_stripes, 65535);
+  uint32_t chunk = kRowChunk16;
+  while (chunk > 4 && tiles * stripes * ((a.rows + chunk - 1) / chunk) < 2ull * sms) chunk /= 2;
+  a.row_chunk = chunk;
+  grid = dim3((unsigned)tiles, stripes, (a.rows + chunk - 1) / chunk);
+}
 
 __device__ __forceinline__ uint2 load_sym8(const uint8_t *p, uint64_t remain) {
   if (remain >= 8 && (((uintptr_t)p & 7u) == 0)) return *reinterpret_cast<const uint2 *>(p);
@@ -303,13 +318,13 @@ __global__ void __launch_bounds__(kThreads) gf16_matrix_kernel(const Apply16Args
   __shared__ __align__(16) uint32_t R[2048];
   fill_rtab(R);
   __syncthreads();
-  const uint64_t sym = ((uint64_t)blockIdx.x * kThreads + threadIdx.x) * 8;
-  const uint32_t k = a.k;
+  const uint64_t sym = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 8;
+  const uint32_t k = a.k, chunk = a.row_chunk;
   for (uint32_t s = blockIdx.y; s < a.n_stripes; s += gridDim.y) {
     if (sym >= a.n_sym) continue;
     const uint64_t remain = a.n_sym - sym;
-    const uint32_t g_end = min(a.rows, (blockIdx.z + 1) * kRowChunk16);
-    for (uint32_t g = blockIdx.z * kRowChunk16; g < g_end; g += OUT_TILE) {
+    const uint32_t g_end = min(a.rows, (blockIdx.z + 1) * chunk);
+    for (uint32_t g = blockIdx.z * chunk; g < g_end; g += OUT_TILE) {
       const uint32_t live = g_end - g;
       uint32_t lo_acc[OUT_TILE][2], hi_acc[OUT_TILE][2];
 #pragma unroll

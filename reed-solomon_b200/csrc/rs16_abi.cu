@@ -12,6 +12,7 @@
 #include "runtime.hpp"
 #include "gf_host.hpp"
 #include "fft16.hpp"
+#include "kernels_fft.cuh"
 #include "kernels_lagrange.cuh"
 #include "kernels_matrix.cuh"
 
@@ -99,12 +100,14 @@ static int lagrange16_device(const std::vector<uint16_t> &nodes, const std::vect
 
 static int launch_gf16(const Apply16Args &a, bool verify, cudaStream_t st) {
   if (a.n_sym == 0 || a.rows == 0 || a.n_stripes == 0) return RS_OK;
-  uint64_t tiles = (a.n_sym + kThreads * 8 - 1) / (kThreads * 8);
-  dim3 grid((unsigned)tiles, std::min<uint32_t>(a.n_stripes, 65535), (a.rows + kRowChunk16 - 1) / kRowChunk16);
+  Apply16Args b = a;
+  dim3 grid;
+  unsigned threads;
+  gf16_launch_shape(b, sm_count(), grid, threads);
   if (verify)
-    gf16_matrix_kernel<4, true><<<grid, kThreads, 0, st>>>(a);
+    gf16_matrix_kernel<4, true><<<grid, threads, 0, st>>>(b);
   else
-    gf16_matrix_kernel<4, false><<<grid, kThreads, 0, st>>>(a);
+    gf16_matrix_kernel<4, false><<<grid, threads, 0, st>>>(b);
   g_launches++;
   RSB_CU(cudaGetLastError());
   return RS_OK;

@@ -360,9 +360,11 @@ static void release_request(rs_server *s, Req &q) {
 
 static int launch_gf16_server(const Apply16Args &a, cudaStream_t st) {
   if (a.n_sym == 0 || a.rows == 0 || a.n_stripes == 0) return RS_OK;
-  uint64_t tiles = (a.n_sym + kThreads * 8 - 1) / (kThreads * 8);
-  dim3 grid((unsigned)tiles, std::min<uint32_t>(a.n_stripes, 65535), (a.rows + kRowChunk16 - 1) / kRowChunk16);
-  gf16_matrix_kernel<4, false><<<grid, kThreads, 0, st>>>(a);
+  Apply16Args b = a;
+  dim3 grid;
+  unsigned threads;
+  gf16_launch_shape(b, sm_count(), grid, threads);
+  gf16_matrix_kernel<4, false><<<grid, threads, 0, st>>>(b);
   g_launches++;
   RSB_CU(cudaGetLastError());
   return RS_OK;

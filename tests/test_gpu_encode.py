@@ -207,3 +207,24 @@ def test_encode_dev_pointers(gpu, O):
         got = np.array([b.cpu().numpy() for b in bufs[k:]])
         assert np.array_equal(got, O.encode8(k, m, host)), route
     assert rs.verify_dev(bufs, length)
+
+
+def test_encode_dev_unaligned_pointers(gpu, O):
+    """Shards at odd byte offsets take the FFT kernel's byte path; same bytes."""
+    import torch
+
+    k, m, length = 16, 16, 4099
+    rs = gpu.ReedSolomon(k, m)
+    host = rand_data(k, length, 78)
+    pool = torch.zeros((k + m) * (length + 64), dtype=torch.uint8, device="cuda")
+    bufs = [pool[i * (length + 64) + 1 + i: i * (length + 64) + 1 + i + length] for i in range(k + m)]
+    for i in range(k):
+        bufs[i].copy_(torch.from_numpy(host[i]))
+    for route in ("matrix", "fft"):
+        rs.set_route(route)
+        for b in bufs[k:]:
+            b.zero_()
+        rs.encode_dev(bufs)
+        torch.cuda.synchronize()
+        got = np.array([b.cpu().numpy() for b in bufs[k:]])
+        assert np.array_equal(got, O.encode8(k, m, host)), route
