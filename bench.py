@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--tuner-workloads", type=int, default=10000,
                     help="workloads the tuner times (about 5 applicable configurations each)")
     ap.add_argument("--requests", type=int, default=400, help="requests of the serve workload")
+    ap.add_argument("--rs16", default=None, help="rs16 workload: one shape K,M,STRIPES instead of both")
     return ap.parse_args()
 
 
@@ -76,7 +77,7 @@ def profile_traffic():
     for line in open(path):
         if line.startswith("dram_bytes_per_stripe:"):
             per_stripe = float(line.split(":")[1])
-    return per_stripe, path
+    return per_stripe, os.path.relpath(path, ROOT)
 
 
 class Clocks:
@@ -318,7 +319,11 @@ def run_workload(args):
             line = {"metric": "mixed-shape batch GB/s, batched+tuned vs plain", "unit": "GB/s",
                     "value": res["batched_gbs"], "results": res}
         elif args.workload == "rs16":
-            res = workloads.rs16_shapes()
+            if args.rs16:
+                k16, m16, n16 = (int(x) for x in args.rs16.split(","))
+                res = workloads.rs16_shapes(shapes=((k16, m16, n16),))
+            else:
+                res = workloads.rs16_shapes()
             line = {"metric": "ReedSolomon16 encode/reconstruct GB/s", "unit": "GB/s", "results": res}
         elif args.workload == "tuner":
             res = workloads.tuner_regret(n_workloads=args.tuner_workloads)

@@ -393,7 +393,7 @@ __device__ __forceinline__ FftLoc fft_locate(const FftArgs &a, uint64_t pair) {
 struct FftVariant {
   int threads, ctas, sync;
 };
-constexpr FftVariant kFftVariants[] = {{128, 3, 0}, {128, 4, 0}};
+constexpr FftVariant kFftVariants[] = {{128, 3, 0}, {128, 4, 0}, {128, 2, 0}};
 constexpr int kFftVariantCount = sizeof(kFftVariants) / sizeof(kFftVariants[0]);
 
 // Per-thread staging of one 32-column group in shared memory: shard slot j, half q
@@ -554,11 +554,11 @@ __global__ void __launch_bounds__(THREADS, CTAS)
   }
 }
 
-// Selected launch shape (index into kFftVariants); set by rs_set_fft_variant.
-// Per-K launch shape (index into kFftVariants), defaults from a sweep on B200:
-// K = 16 and 64 prefer 4 CTAs/SM, the others 3.
+// Per-K launch shape (index into kFftVariants), defaults from a sweep on B200 (128
+// stripes of 1 MiB shards): K = 8 and 16 prefer 4 CTAs/SM, K = 32 and 64 two (their
+// 255-register ceiling removes spills), K = 128 three.
 inline int &fft_variant_for(int K) {
-  static int v[8] = {0, 0, 0, 0, 1, 0, 1, 0};
+  static int v[8] = {0, 0, 0, 1, 1, 2, 2, 0};
   int l = 0;
   while ((1 << l) < K) l++;
   return v[l & 7];
@@ -592,7 +592,7 @@ constexpr int fft_w_hi(int K) { return K <= 8 ? 1 : K <= 32 ? 2 : K == 64 ? 3 : 
 
 // Selected lane-group width per K: 0 = fft_w_lo, 1 = fft_w_hi (rs_set_fft_lanes).
 inline int &fft_lanes_choice(int K) {
-  static int c[8] = {0, 0, 0, 0, 0, 0, 1, 0};  // wide groups only for K = 64
+  static int c[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // narrow groups measured fastest for every K
   int l = 0;
   while ((1 << l) < K) l++;
   return c[l & 7];
@@ -620,6 +620,7 @@ inline cudaError_t launch_fft_kw(const FftArgs &a, const PtrTableT<PTRS> &pt, cu
     return launch_fft_kwv<K, W, PTRS, 0>(a, pt, st);  // single-stripe calls
   } else {
     if (fft_variant_for(K) == 1) return launch_fft_kwv<K, W, PTRS, 1>(a, pt, st);
+    if (fft_variant_for(K) == 2) return launch_fft_kwv<K, W, PTRS, 2>(a, pt, st);
     return launch_fft_kwv<K, W, PTRS, 0>(a, pt, st);
   }
 }

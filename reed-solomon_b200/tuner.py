@@ -8,7 +8,7 @@ shapes, never arithmetic, so every choice yields the same bytes.
 
 Candidates (GF(2^8)):
   matrix route, tile variant 0..3 (parity rows per thread x output rows per CTA)
-  FFT route ((K,K) shapes), lane-group width narrow/wide x CTAs per SM 3/4
+  FFT route ((K,K) shapes), lane-group width narrow/wide x CTAs per SM 3/4/2
 """
 import ctypes
 import math
@@ -19,7 +19,8 @@ from . import _lib
 from .coder import ReedSolomon, _check
 
 CONFIGS = [("matrix", 0), ("matrix", 1), ("matrix", 2), ("matrix", 3),
-           ("fft", (0, 0)), ("fft", (0, 1)), ("fft", (1, 0)), ("fft", (1, 1))]
+           ("fft", (0, 0)), ("fft", (0, 1)), ("fft", (1, 0)), ("fft", (1, 1)),
+           ("fft", (0, 2)), ("fft", (1, 2))]
 N_FEATURES = 5
 FFT_K = (2, 4, 8, 16, 32, 64, 128)
 
@@ -240,7 +241,7 @@ class CostModel:
         return P.argmin(axis=1)
 
 
-DEFAULT_FFT = {2: (0, 0), 4: (0, 0), 8: (0, 0), 16: (0, 1), 32: (0, 0), 64: (1, 1), 128: (0, 0)}
+DEFAULT_FFT = {2: (0, 0), 4: (0, 0), 8: (0, 1), 16: (0, 1), 32: (0, 2), 64: (0, 2), 128: (0, 0)}
 
 
 def default_choice(workloads, T):
