@@ -102,7 +102,7 @@ __device__ __forceinline__ void store_reg16(uint32_t *p, const Reg16 &r) {
 // LV = 1: registers {i0, i0+h} at level L (h = 2^L). LV = 2: {i0, i0+h, i0+2h, i0+3h},
 // levels L and L+1 (inverse: L then L+1; forward: L+1 then L).
 template <int LV>
-__global__ void __launch_bounds__(kFft16Threads) fft16_pass_kernel(const Fft16PassArgs a) {
+__global__ void __launch_bounds__(kFft16Threads, 2) fft16_pass_kernel(const Fft16PassArgs a) {
   constexpr int NC = LV == 2 ? 3 : 1;
   __shared__ __align__(16) uint32_t mk[NC][256];
   const uint32_t R = a.R, L = a.level, h = 1u << L;
