@@ -324,8 +324,9 @@ void rs16_dec_free(rs16_dec_t *dec);
  * LCH transform, src/fft16.rs; k a power of two, any m, picked when its estimated work
  * is below the matrix kernel's) or "matrix". */
 const char *rs16_encode_route(const rs16_t *codec);
-/* Forced-route test hook like rs8_set_route: 0 automatic, 1 matrix, 2 FFT where the
- * shape has it (k a power of two >= 2). Both routes give identical bytes. */
+/* Forced-route test hook like rs8_set_route: 0 automatic, 1 matrix, 2 FFT (encode for
+ * k >= 2; reconstruct plans built afterwards use the FFT erasure decoder). Both routes
+ * give identical bytes. */
 int rs16_set_route(rs16_t *codec, int route);
 int rs16_encode_dev(rs16_t *codec, uint8_t *const *d_shards, size_t n_shards, size_t len,
                     void *stream);

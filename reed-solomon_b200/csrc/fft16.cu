@@ -140,6 +140,138 @@ bool fft16_build(size_t k, size_t m, Fft16Program &p) {
   return true;
 }
 
+bool fft16_decode_build(size_t k, size_t m, const std::vector<uint32_t> &survivors,
+                        const std::vector<uint32_t> &targets, Fft16Decode &d) {
+  const size_t n = k + m;
+  if (k < 1 || n > 65536 || survivors.size() != k || targets.empty()) return false;
+  d = Fft16Decode{};
+  d.n = (uint32_t)n;
+  uint32_t N = 2;
+  while (N < n) N <<= 1;
+  d.N = N;
+  d.lg = (uint32_t)log2_exact(N);
+  d.targets = targets;
+  // Log-domain XOR-convolution conv[x] = sum_{e in E} log(x ^ e) (log 0 taken as 0),
+  // by Walsh-Hadamard transforms in wrapping 64-bit arithmetic: the true sums are
+  // below 2^32 and N <= 2^16, so N * conv is exact modulo 2^64.
+  const Gf16Tables &T = gf16();
+  std::vector<uint64_t> a(N, 1), b(N, 0);
+  for (uint32_t s : survivors) a[s] = 0;
+  for (uint32_t x = 1; x < N; x++) b[x] = T.log[x];
+  auto fwht = [N](std::vector<uint64_t> &v) {
+    for (uint32_t h = 1; h < N; h <<= 1)
+      for (uint32_t i = 0; i < N; i += 2 * h)
+        for (uint32_t j = i; j < i + h; j++) {
+          const uint64_t x = v[j], y = v[j + h];
+          v[j] = x + y;
+          v[j + h] = x - y;
+        }
+  };
+  fwht(a);
+  fwht(b);
+  for (uint32_t x = 0; x < N; x++) a[x] *= b[x];
+  fwht(a);
+  auto locator = [&](uint32_t x) { return T.exp[(a[x] / N) % 65535]; };
+  auto push16 = [&](uint16_t c) {
+    for (int p = 0; p < 16; p++) d.cols.push_back(gf16_mul(c, (uint16_t)(1u << p)));
+  };
+  // Transform constants (beta 0, both directions): (l, j) at N - (N >> l) + j.
+  for (uint32_t l = 0; l < d.lg; l++)
+    for (uint32_t j = 0; j < (N >> (l + 1)); j++) push16(what16()((int)l, (uint16_t)(j << (l + 1))));
+  // Row scales: L at the survivors, 0 elsewhere.
+  d.row_off = d.cols.size() / 16;
+  std::vector<uint16_t> scale(N, 0);
+  for (uint32_t s : survivors) scale[s] = locator(s);
+  for (uint32_t x = 0; x < N; x++) push16(scale[x]);
+  // kappa_t = (product of the nonzero points of V_t) / W_t(2^t), since
+  // W_t(x) = x * prod_{a in V_t, a != 0} (x - a).
+  d.kappa_off = d.cols.size() / 16;
+  uint16_t prod = 1;
+  for (uint32_t t = 0; t < d.lg; t++) {
+    push16(gf16_mul(prod, what16().pivot_inv[t]));
+    for (uint32_t x = (1u << t); x < (2u << t); x++) prod = gf16_mul(prod, (uint16_t)x);
+  }
+  // Target scales: 1 / L'(e).
+  d.target_off = d.cols.size() / 16;
+  for (uint32_t e : targets) push16(gf16_inv(locator(e)));
+  d.butterflies = (uint64_t)3 * (N / 2) * d.lg + N + targets.size();
+  return true;
+}
+
+bool fft16_decode_preferred(const Fft16Decode &d, size_t k) {
+  // LOP3 per 32-symbol group: a butterfly or scaled row about 290, counted twice for
+  // the passes' L2 traffic; the matrix route 208 per coefficient plus about as much
+  // again to build its rows.
+  const double fft = 2.0 * 290.0 * (double)d.butterflies;
+  const double matrix = 2.0 * 208.0 * (double)d.targets.size() * k;
+  return fft < matrix;
+}
+
+size_t fft16_decode_scratch_bytes(const Fft16Decode &d, size_t len, size_t budget) {
+  const uint64_t G = (len / 2 + 31) / 32, per_group = (uint64_t)d.regs() * 64;
+  return (size_t)std::max<uint64_t>(per_group, std::min<uint64_t>(G * per_group, budget / per_group * per_group));
+}
+
+int fft16_decode_run(const Fft16Decode &d, const uint16_t *d_cols, uint8_t *scratch, size_t scratch_bytes,
+                     uint8_t *const *d_ptrs, const uint32_t *d_targets, size_t n_targets, size_t len,
+                     cudaStream_t st) {
+  if (n_targets == 0) return RS_OK;
+  const uint32_t N = d.N;
+  const uint64_t Nsym = len / 2, G = (Nsym + 31) / 32, per_group = (uint64_t)d.regs() * 64;
+  if (scratch_bytes < per_group) return RS_ERR_TOO_LARGE;
+  const uint64_t gc = std::min<uint64_t>(G, scratch_bytes / per_group);
+  for (uint64_t g0 = 0; g0 < G; g0 += gc) {
+    const uint64_t gn = std::min<uint64_t>(gc, G - g0);
+    uint32_t *C = reinterpret_cast<uint32_t *>(scratch), *W = C + (uint64_t)N * gn * 16;
+    const unsigned rthreads = (unsigned)std::min<uint64_t>(kFft16Threads, (gn + 31) / 32 * 32);
+    fft16_scale_load_kernel<<<N, rthreads, 0, st>>>(d_ptrs, d_cols + d.row_off * 16, d.n, Nsym, g0, gn, C);
+    g_launches++;
+    RSB_CU(cudaGetLastError());
+    // Transforms of N registers at beta 0: inverse on C (levels 0, 1 | 2, 3 | ..., an
+    // odd top level alone); the forward one on W mirrors it.
+    auto pass = [&](uint32_t *buf, int level, int lv, bool inverse) -> int {
+      Fft16PassArgs a{};
+      a.src = buf;
+      a.dst = buf;
+      a.cols = d_cols;
+      a.R = N;
+      a.level = (uint32_t)level;
+      a.src_regs = a.dst_regs = N;
+      a.G = gn;
+      a.n_stripes = 1;
+      a.inverse = inverse;
+      const uint64_t tasks = (gn + 31) / 32;
+      const unsigned threads = (unsigned)(32 * std::min<uint64_t>(8, tasks));
+      const unsigned gy = (unsigned)std::min<uint64_t>(65535, (tasks * 32 + threads - 1) / threads);
+      if (lv == 2)
+        fft16_pass_kernel<2><<<dim3(N / 4, gy), threads, 0, st>>>(a);
+      else
+        fft16_pass_kernel<1><<<dim3(N / 2, gy), threads, 0, st>>>(a);
+      g_launches++;
+      RSB_CU(cudaGetLastError());
+      return RS_OK;
+    };
+    const int lg = (int)d.lg;
+    int L = 0;
+    for (; L + 1 < lg; L += 2) RSB_TRY(pass(C, L, 2, true));
+    if (L < lg) RSB_TRY(pass(C, L, 1, true));
+    fft16_derivative_kernel<<<N, rthreads, 0, st>>>(C, W, d_cols + d.kappa_off * 16, d.lg, gn);
+    g_launches++;
+    RSB_CU(cudaGetLastError());
+    int top = lg - 1;
+    if (lg % 2 == 1) {
+      RSB_TRY(pass(W, top, 1, false));
+      top--;
+    }
+    for (int l = top - 1; l >= 0; l -= 2) RSB_TRY(pass(W, l, 2, false));
+    fft16_scale_store_kernel<<<(unsigned)std::min(n_targets, d.targets.size()), rthreads, 0, st>>>(
+        W, d_targets, d_cols + d.target_off * 16, d_ptrs, Nsym, g0, gn);
+    g_launches++;
+    RSB_CU(cudaGetLastError());
+  }
+  return RS_OK;
+}
+
 bool fft16_preferred(const Fft16Program &p) {
   // LOP3 per 32-symbol group: the matrix kernel about 208 per coefficient, a butterfly
   // about 290; the FFT's passes also move scratch through L2 (counted as 2x).

@@ -54,6 +54,38 @@ struct Fft16Program {
   uint32_t regs() const { return t + regs_s() + regs_w(); }  // per stripe and group
 };
 
+// Erasure decoding on the FFT route for one presence pattern (one stripe per run).
+// With N the power of two >= n shards, the code is f (degree < k) evaluated at points
+// 0..n-1. Only the k survivors are read; every other point of {0..N-1} is treated as
+// erased (E). With the error locator L(x) = prod_{e in E} (x - e), g = f * L has
+// degree < N and is known everywhere: f(i) L(i) at survivors, 0 on E. An inverse
+// transform gives g's novel-basis coefficients, the formal derivative there is
+// D(X_i) = sum_{t in bits(i)} kappa_t X_{i - 2^t} (each normalised subspace polynomial
+// is linearized, so its derivative is a constant kappa_t), a forward transform gives g'
+// everywhere, and at an erased point f(e) = g'(e) / L'(e). L at the survivors and L' on
+// E are one XOR-convolution of E's indicator with the discrete log table.
+struct Fft16Decode {
+  uint32_t n = 0, N = 0, lg = 0;
+  std::vector<uint32_t> targets;  // points to rebuild, in output order
+  std::vector<uint16_t> cols;     // transform (N-1) | row scale (N) | kappa (lg) | targets
+  uint64_t row_off = 0, kappa_off = 0, target_off = 0;
+  uint64_t butterflies = 0;       // per 32-symbol group (route estimate)
+  uint32_t regs() const { return 2 * N; }  // C + W per group
+};
+
+// survivors: the k points read; targets: the points to rebuild (k + m <= 65536).
+bool fft16_decode_build(size_t k, size_t m, const std::vector<uint32_t> &survivors,
+                        const std::vector<uint32_t> &targets, Fft16Decode &d);
+// Whether the decode's estimated work is below the matrix route's (rows x k
+// coefficients plus building those rows).
+bool fft16_decode_preferred(const Fft16Decode &d, size_t k);
+size_t fft16_decode_scratch_bytes(const Fft16Decode &d, size_t len, size_t budget);
+// d_ptrs: device table of the n shard pointers (survivors read, targets written);
+// d_targets: the target points on the device, of which the first n_targets are stored.
+int fft16_decode_run(const Fft16Decode &d, const uint16_t *d_cols, uint8_t *scratch, size_t scratch_bytes,
+                     uint8_t *const *d_ptrs, const uint32_t *d_targets, size_t n_targets, size_t len,
+                     cudaStream_t st);
+
 // False (no FFT route) for k < 2.
 bool fft16_build(size_t k, size_t m, Fft16Program &p);
 // Whether the FFT route's estimated work is below the tower matrix kernel's.

@@ -243,4 +243,106 @@ __global__ void __launch_bounds__(kFft16Threads)
   }
 }
 
+// ---- erasure decoding on the FFT route (one stripe, shards through a pointer table) ----
+//
+// Masks of one constant from its 16 columns into shared memory (all threads of the CTA).
+__device__ __forceinline__ void masks_from_cols(uint32_t *mk, const uint16_t *cols) {
+  for (uint32_t t = threadIdx.x; t < 256; t += blockDim.x) mk[t] = ((cols[t & 15] >> (t >> 4)) & 1) ? ~0u : 0u;
+}
+
+// d = M * s (product only)
+__device__ __forceinline__ void mul16_set(Reg16 &d, const Reg16 &s, const uint32_t *m) {
+#pragma unroll
+  for (int b = 0; b < 16; b++) d[b] = 0;
+  mul16_acc(d, s, m);
+}
+
+// Register r of C (one CTA per register, N of them): the shard at point r times its
+// constant c_r (cols + 16 r), or zero where c_r = 0 (erased points and padding past
+// the last shard, whose pointer is not read). Symbol groups g0 .. g0+G-1.
+__global__ void __launch_bounds__(kFft16Threads)
+    fft16_scale_load_kernel(const uint8_t *const *ptrs, const uint16_t *cols, uint32_t n, uint64_t Nsym,
+                            uint64_t g0, uint64_t G, uint32_t *dst) {
+  __shared__ __align__(16) uint32_t mk[256];
+  __shared__ int live;
+  const uint32_t r = blockIdx.x;
+  const uint16_t *c = cols + 16 * (uint64_t)r;
+  if (threadIdx.x == 0) {
+    int any = 0;
+    for (int p = 0; p < 16; p++) any |= c[p];
+    live = r < n && any;
+  }
+  masks_from_cols(mk, c);
+  __syncthreads();
+  for (uint64_t g = threadIdx.x; g < G; g += blockDim.x) {
+    Reg16 y;
+    if (live) {
+      const uint8_t *row = ptrs[r];
+      const uint64_t col = (g0 + g) * 32, remain = Nsym - col;
+      uint32_t lo[8], hi[8];
+      load32(row + col, remain, lo);
+      load32(row + Nsym + col, remain, hi);
+      bit_transpose(lo);
+      bit_transpose(hi);
+      Reg16 x;
+#pragma unroll
+      for (int i = 0; i < 8; i++) x[i] = lo[i], x[8 + i] = hi[i];
+      mul16_set(y, x, mk);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; i++) y[i] = 0;
+    }
+    store_reg16(dst + ((uint64_t)r * G + g) * 16, y);
+  }
+}
+
+// Formal derivative in the novel basis (one CTA per output register j < N):
+// D_j = sum over levels t with bit t of j clear of kappa_t * C_{j + 2^t}, kappa_t the
+// constant derivative of the normalised subspace polynomial of level t.
+__global__ void __launch_bounds__(kFft16Threads)
+    fft16_derivative_kernel(const uint32_t *src, uint32_t *dst, const uint16_t *kcols, uint32_t lg, uint64_t G) {
+  __shared__ __align__(16) uint32_t mk[16][256];
+  const uint32_t j = blockIdx.x;
+  for (uint32_t t = threadIdx.x; t < lg * 256; t += blockDim.x)
+    mk[t >> 8][t & 255] = ((kcols[16 * (t >> 8) + (t & 15)] >> ((t >> 4) & 15)) & 1) ? ~0u : 0u;
+  __syncthreads();
+  for (uint64_t g = threadIdx.x; g < G; g += blockDim.x) {
+    Reg16 acc;
+#pragma unroll
+    for (int i = 0; i < 16; i++) acc[i] = 0;
+    for (uint32_t t = 0; t < lg; t++) {
+      if ((j >> t) & 1) continue;
+      Reg16 x;
+      load_reg16(src + ((uint64_t)(j + (1u << t)) * G + g) * 16, x);
+      mul16_acc(acc, x, mk[t]);
+    }
+    store_reg16(dst + ((uint64_t)j * G + g) * 16, acc);
+  }
+}
+
+// Rebuilt shards (one CTA per target i): point rows[i] of W times its constant
+// (tcols + 16 i), back to bytes at ptrs[rows[i]].
+__global__ void __launch_bounds__(kFft16Threads)
+    fft16_scale_store_kernel(const uint32_t *src, const uint32_t *rows, const uint16_t *tcols,
+                             uint8_t *const *ptrs, uint64_t Nsym, uint64_t g0, uint64_t G) {
+  __shared__ __align__(16) uint32_t mk[256];
+  const uint32_t i = blockIdx.x, r = rows[i];
+  masks_from_cols(mk, tcols + 16 * (uint64_t)i);
+  __syncthreads();
+  uint8_t *row = ptrs[r];
+  for (uint64_t g = threadIdx.x; g < G; g += blockDim.x) {
+    Reg16 x, y;
+    load_reg16(src + ((uint64_t)r * G + g) * 16, x);
+    mul16_set(y, x, mk);
+    uint32_t lo[8], hi[8];
+#pragma unroll
+    for (int b = 0; b < 8; b++) lo[b] = y[b], hi[b] = y[8 + b];
+    bit_transpose(lo);
+    bit_transpose(hi);
+    const uint64_t col = (g0 + g) * 32, remain = Nsym - col;
+    store32(row + col, remain, lo);
+    store32(row + Nsym + col, remain, hi);
+  }
+}
+
 }  // namespace rsb

@@ -149,8 +149,9 @@ namespace rsb {
 
 // Plan of one presence pattern: closed-form Lagrange rows from the survivors to each
 // missing shard (data ascending, then parity ascending), built on the device.
+// route: 0 by estimated cost, 1 matrix (Lagrange rows), 2 FFT decode.
 static int plan16_for(const Gen16 &g, PlanCache &cache, const Presence &pres,
-                      std::shared_ptr<const Plan> &out) {
+                      std::shared_ptr<const Plan> &out, int route = 0) {
   out = cache.find(pres);
   if (out) return RS_OK;
   auto plan = std::make_shared<Plan>();
@@ -162,6 +163,24 @@ static int plan16_for(const Gen16 &g, PlanCache &cache, const Presence &pres,
   std::vector<uint16_t> targets(plan->missing_data.begin(), plan->missing_data.end());
   targets.insert(targets.end(), plan->missing_parity.begin(), plan->missing_parity.end());
   RSB_CU(cudaSetDevice(g.device));
+  // FFT-route decode where its estimated work is lower than the matrix route's.
+  if (!targets.empty()) {
+    auto dec = std::make_shared<Fft16Decode>();
+    std::vector<uint32_t> t32(targets.begin(), targets.end());
+    if (route != 1 && fft16_decode_build(g.k, g.m, plan->survivors, t32, *dec) &&
+        (route == 2 || fft16_decode_preferred(*dec, g.k))) {
+      const size_t cbytes = dec->cols.size() * 2, toff = (cbytes + 15) & ~size_t(15);
+      void *d = nullptr;
+      RSB_CU(cudaMalloc(&d, toff + t32.size() * 4));
+      plan->d_rows = d;
+      RSB_CU(cudaMemcpy(d, dec->cols.data(), cbytes, cudaMemcpyHostToDevice));
+      RSB_CU(cudaMemcpy(static_cast<uint8_t *>(d) + toff, t32.data(), t32.size() * 4, cudaMemcpyHostToDevice));
+      plan->fft16 = dec;
+      plan->fft16_targets_off = toff;
+      out = cache.insert(pres, plan);
+      return RS_OK;
+    }
+  }
   uint32_t *d = nullptr;
   int st = lagrange16_device(nodes, targets, &d);
   plan->d_rows = d;
@@ -195,7 +214,48 @@ static int apply16_ptrs(const uint32_t *coeffs, uint32_t k, uint32_t rows, const
   return st_;
 }
 
-static int reconstruct16(const Gen16 &g, PlanCache *cache, const Plan *fixed, Exec &ex,
+// Rebuilds the first `rows` targets of an FFT-route plan (missing data first, then
+// missing parity). Device shards go through a stream-ordered pointer table; host shards
+// are staged: survivors copied in, rebuilt rows copied back.
+static int fft16_reconstruct(const Gen16 &g, const Plan &plan, Exec &ex, uint8_t *const *shards, size_t len,
+                             size_t rows, bool dev, cudaStream_t st) {
+  const Fft16Decode &d = *plan.fft16;
+  const size_t n = g.k + g.m;
+  const uint16_t *d_cols = static_cast<const uint16_t *>(plan.d_rows);
+  const uint32_t *d_targets =
+      reinterpret_cast<const uint32_t *>(static_cast<const uint8_t *>(plan.d_rows) + plan.fft16_targets_off);
+  const size_t sbytes = fft16_decode_scratch_bytes(d, len, kFft16ScratchBudget);
+  RSB_CU(cudaSetDevice(g.device));
+  if (dev) {
+    uint8_t *mem = nullptr;
+    const size_t tbytes = (n * sizeof(void *) + 255) & ~size_t(255);
+    RSB_CU(cudaMallocAsync(&mem, tbytes + sbytes, st));
+    int rc = RS_OK;
+    if (cudaMemcpyAsync(mem, shards, n * sizeof(void *), cudaMemcpyHostToDevice, st) != cudaSuccess) rc = RS_ERR_CUDA;
+    if (rc == RS_OK)
+      rc = fft16_decode_run(d, d_cols, mem + tbytes, sbytes, reinterpret_cast<uint8_t *const *>(mem), d_targets,
+                            rows, len, st);
+    cudaFreeAsync(mem, st);
+    return rc;
+  }
+  std::lock_guard<std::mutex> lock(ex.mu);
+  const size_t tbytes = (n * sizeof(void *) + 255) & ~size_t(255);
+  RSB_TRY(ex.buf.ensure(n * len));
+  RSB_TRY(ex.aux.ensure(tbytes + sbytes));
+  std::vector<uint8_t *> ptrs(n);
+  for (size_t i = 0; i < n; i++) ptrs[i] = ex.buf.ptr + i * len;
+  for (uint32_t s : plan.survivors)
+    RSB_CU(cudaMemcpyAsync(ptrs[s], shards[s], len, cudaMemcpyHostToDevice, ex.stream));
+  RSB_CU(cudaMemcpyAsync(ex.aux.ptr, ptrs.data(), n * sizeof(void *), cudaMemcpyHostToDevice, ex.stream));
+  RSB_TRY(fft16_decode_run(d, d_cols, ex.aux.ptr + tbytes, sbytes, reinterpret_cast<uint8_t *const *>(ex.aux.ptr),
+                           d_targets, rows, len, ex.stream));
+  for (size_t j = 0; j < rows; j++)
+    RSB_CU(cudaMemcpyAsync(shards[d.targets[j]], ptrs[d.targets[j]], len, cudaMemcpyDeviceToHost, ex.stream));
+  RSB_CU(cudaStreamSynchronize(ex.stream));
+  return RS_OK;
+}
+
+static int reconstruct16(const Gen16 &g, PlanCache *cache, const Plan *fixed, Exec &ex, int route,
                          uint8_t *const *shards, const size_t *lens, const uint8_t *present,
                          size_t n_shards, bool data_only, bool dev, cudaStream_t st) {
   size_t n = g.k + g.m;
@@ -211,7 +271,7 @@ static int reconstruct16(const Gen16 &g, PlanCache *cache, const Plan *fixed, Ex
   std::shared_ptr<const Plan> hold;
   const Plan *plan = fixed;
   if (!plan) {
-    RSB_TRY(plan16_for(g, *cache, pres, hold));
+    RSB_TRY(plan16_for(g, *cache, pres, hold, route));
     plan = hold.get();
   }
   RSB_TRY(check_absent_buffers(lens, present, n, g.k, len, data_only));
@@ -219,6 +279,7 @@ static int reconstruct16(const Gen16 &g, PlanCache *cache, const Plan *fixed, Ex
   if (rows == 0) return RS_OK;
   std::vector<uint32_t> outs(plan->missing_data);
   if (!data_only) outs.insert(outs.end(), plan->missing_parity.begin(), plan->missing_parity.end());
+  if (plan->fft16) return fft16_reconstruct(g, *plan, ex, shards, len, rows, dev, st);
   const uint32_t *coeffs = reinterpret_cast<const uint32_t *>(plan->d_rows);
   if (dev) {
     RSB_CU(cudaSetDevice(g.device));
@@ -428,7 +489,7 @@ int rs16_verify(rs16_t *c, const uint8_t *const *shards, size_t n_shards, size_t
 int rs16_reconstruct(rs16_t *c, uint8_t *const *shards, const size_t *lens, const uint8_t *present,
                      size_t n_shards, int data_only) {
   if (!c) return RS_ERR_INVALID_ARGUMENT;
-  return reconstruct16(*c->gen, c->plans.get(), nullptr, *c->exec, shards, lens, present, n_shards,
+  return reconstruct16(*c->gen, c->plans.get(), nullptr, *c->exec, c->route.load(), shards, lens, present, n_shards,
                        data_only != 0, false, nullptr);
 }
 
@@ -464,7 +525,7 @@ int rs16_prepare_decode(rs16_t *c, const uint8_t *present, size_t n_present, rs1
     }
   if (count < g.k) return RS_TOO_FEW_SHARDS_PRESENT;
   std::shared_ptr<const Plan> plan;
-  RSB_TRY(plan16_for(g, *c->plans, pres, plan));
+  RSB_TRY(plan16_for(g, *c->plans, pres, plan, c->route.load()));
   auto d = new (std::nothrow) rs16_decoder();
   if (!d) return RS_ERR_ALLOC;
   d->gen = c->gen;
@@ -477,7 +538,7 @@ int rs16_prepare_decode(rs16_t *c, const uint8_t *present, size_t n_present, rs1
 int rs16_dec_reconstruct(rs16_dec_t *d, uint8_t *const *shards, const size_t *lens, const uint8_t *present,
                          size_t n_shards, int data_only) {
   if (!d) return RS_ERR_INVALID_ARGUMENT;
-  return reconstruct16(*d->gen, nullptr, d->plan.get(), *d->exec, shards, lens, present, n_shards,
+  return reconstruct16(*d->gen, nullptr, d->plan.get(), *d->exec, 0, shards, lens, present, n_shards,
                        data_only != 0, false, nullptr);
 }
 
@@ -539,7 +600,7 @@ int rs16_encode_batch_dev(rs16_t *c, const uint8_t *d_data, size_t data_stride, 
 int rs16_reconstruct_dev(rs16_t *c, uint8_t *const *d_shards, const size_t *lens, const uint8_t *present,
                          size_t n_shards, int data_only, void *stream) {
   if (!c) return RS_ERR_INVALID_ARGUMENT;
-  return reconstruct16(*c->gen, c->plans.get(), nullptr, *c->exec, d_shards, lens, present, n_shards,
+  return reconstruct16(*c->gen, c->plans.get(), nullptr, *c->exec, c->route.load(), d_shards, lens, present, n_shards,
                        data_only != 0, true, (cudaStream_t)stream);
 }
 

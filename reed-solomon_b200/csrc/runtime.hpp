@@ -107,11 +107,17 @@ struct Presence {
 // One erasure pattern's plan: survivors (first k present, ascending), the missing
 // indexes (data ascending, then parity ascending) and device rows mapping the
 // survivors to each missing shard, in that order.
+struct Fft16Decode;
+
 struct Plan {
   Presence presence;
   std::vector<uint32_t> survivors, missing_data, missing_parity;
   int device = 0;
   void *d_rows = nullptr;  // rows x k coefficients (u8 for GF(2^8), split u32 for the tower)
+  // Tower patterns decoded on the FFT route instead: the decode program; d_rows then
+  // holds its constants followed by its target points (u32).
+  std::shared_ptr<const Fft16Decode> fft16;
+  uint64_t fft16_targets_off = 0;  // byte offset of the target points in d_rows
   ~Plan() {
     if (d_rows) {
       cudaSetDevice(device);

@@ -110,3 +110,78 @@ def test_route_choice(gpu):
     assert gpu.ReedSolomon16(2, 1).encode_route() == "matrix"
     assert gpu.ReedSolomon16(256, 256).encode_route() == "fft"
     assert gpu.ReedSolomon16(300, 500).encode_route() == "fft"
+
+
+def _erase(full, erased):
+    shards = [s.copy() for s in full]
+    for e in erased:
+        shards[e][:] = 0
+    return shards
+
+
+@pytest.mark.parametrize("k,m", [(2, 1), (3, 2), (4, 4), (7, 13), (16, 16), (33, 31), (100, 50), (17, 200),
+                                 (300, 200)])
+def test_fft_decode_rebuilds_every_pattern(gpu, O, k, m):
+    """Erasure decoding on the FFT route (error locator, formal derivative) gives back
+    the original shards for random patterns of 1..m erasures, and data-only leaves the
+    absent parity untouched."""
+    rs = gpu.ReedSolomon16(k, m)
+    rs.set_route("fft")
+    rng = np.random.default_rng(k * 7 + m)
+    n = k + m
+    for length in [2, 66, 1026]:
+        if k * m * length > 40_000_000:
+            continue
+        data = _rand(k, length, length + k)
+        full = np.concatenate([data, O.encode16(k, m, data)])
+        patterns = [[0], [k - 1], list(range(k, n)), list(range(min(m, k)))]
+        patterns += [sorted(rng.choice(n, size=int(rng.integers(1, m + 1)), replace=False).tolist())
+                     for _ in range(4)]
+        for erased in patterns:
+            shards = _erase(full, erased)
+            rs.reconstruct([(s, i not in erased) for i, s in enumerate(shards)])
+            assert np.array_equal(np.array(shards), full), (k, m, length, erased)
+            shards = _erase(full, erased)
+            rs.reconstruct_data([(s, i not in erased) for i, s in enumerate(shards)])
+            for i in range(n):
+                want = full[i] if (i < k or i not in erased) else np.zeros(length, np.uint8)
+                assert np.array_equal(shards[i], want), (k, m, length, erased, i)
+
+
+def test_fft_decode_device_and_large(gpu):
+    """Device-resident shards; (1024,1024) and (4096,12288) with m erasures, FFT decode
+    against the matrix route."""
+    import torch
+
+    for k, m, S in [(1024, 1024, 2048), (4096, 12288, 2048), (1000, 3000, 66)]:
+        n = k + m
+        rs = gpu.ReedSolomon16(k, m)
+        g = torch.Generator(device="cuda").manual_seed(k)
+        rows = torch.zeros((n, S), dtype=torch.uint8, device="cuda")
+        rows[:k] = torch.randint(0, 256, (k, S), dtype=torch.uint8, device="cuda", generator=g)
+        rs.encode_batch_dev(rows[:k], rows[k:], S, 1)
+        torch.cuda.synchronize()
+        full = rows.clone()
+        present = np.ones(n, np.uint8)
+        present[np.random.default_rng(k).choice(n, size=m, replace=False)] = 0
+        for route in ("fft", "matrix"):
+            rs2 = gpu.ReedSolomon16(k, m)
+            rs2.set_route(route)
+            work = full.clone()
+            work[torch.from_numpy(present == 0).cuda()] = 0
+            rs2.reconstruct_dev([work[i] for i in range(n)], present.tolist(), S)
+            torch.cuda.synchronize()
+            assert torch.equal(work, full), (k, m, route)
+
+
+def test_decode_route_choice(gpu, O):
+    """The automatic choice takes the FFT decoder where many shards are rebuilt over
+    many survivors, and still rebuilds exactly."""
+    k, m, length = 512, 512, 64
+    rs = gpu.ReedSolomon16(k, m)
+    data = _rand(k, length, 5)
+    full = np.concatenate([data, O.encode16(k, m, data)])
+    erased = list(range(0, 2 * k, 2))  # every other shard: 512 erasures
+    shards = _erase(full, erased)
+    rs.reconstruct([(s, i not in erased) for i, s in enumerate(shards)])
+    assert np.array_equal(np.array(shards), full)
