@@ -140,6 +140,8 @@ struct Req {
   size_t table_host_off = 0;  // GF(2^8) rows to upload, inside the pinned image
   std::shared_ptr<const Fft16Program> fft16;      // GF(2^16) encode on the FFT route
   std::shared_ptr<const Fft16Program> candidate;  // its program, built at submit
+  std::shared_ptr<const Fft16Decode> dec;         // GF(2^16) reconstruct on the FFT route
+  std::shared_ptr<const Fft16Decode> dec_candidate;
   size_t scratch_budget = 0;                       // FFT scratch limit
 };
 
@@ -223,6 +225,10 @@ static void size_request(Req &q, bool new_table) {
         up += up256(k * 2) + up256(m * 2);                 // nodes | targets
         dev += up256(k * 2) + up256(m * 2) + up256(m * 4);  // w | ell | hit
       }
+    } else if (q.dec) {
+      // constants | target points | pointer table; decode scratch
+      up += up256(q.dec->cols.size() * 2) + up256(e * 4) + up256((k + m) * sizeof(void *));
+      dev += up256(fft16_decode_scratch_bytes(*q.dec, r.row_len, q.scratch_budget));
     } else {
       up += up256(k * 2) + up256(e * 2) + up256((k + e) * sizeof(void *));  // nodes | targets | ptrs
       dev += up256(k * 2) + up256(e * 2) + up256(e * 4) + up256(e * k * 4);  // w | ell | hit | rows
@@ -300,6 +306,13 @@ static bool reserve(rs_server *s, Req &q) {
         if (up256(q.up_bytes) + up256(q.dev_bytes) + up256(fft16_table_bytes(*q.fft16)) > s->cfg.arena_bytes)
           q.fft16.reset();
       }
+    }
+  }
+  if (r.field == 16 && r.op != RS_BATCH_ENCODE) {
+    q.dec = q.dec_candidate;
+    if (q.dec) {
+      size_request(q, false);
+      if (up256(q.up_bytes) + up256(q.dev_bytes) > s->cfg.arena_bytes) q.dec.reset();
     }
   }
   size_request(q, new_table);
@@ -621,6 +634,22 @@ static int enqueue_gf16(rs_server *s, Group &g, cudaStream_t st) {
     a.out_row_stride = r.row_len;
     a.coeffs = reinterpret_cast<const uint32_t *>(s->arena + q.table->span.off);
     a.rows = (uint32_t)m;
+  } else if (q.dec) {
+    if (e == 0) return RS_OK;
+    const Fft16Decode &dd = *q.dec;
+    const size_t cb = up256(dd.cols.size() * 2), tb = up256(e * 4);
+    memcpy(h, dd.cols.data(), dd.cols.size() * 2);
+    uint32_t *tg = reinterpret_cast<uint32_t *>(h + cb);
+    for (size_t j = 0; j < e; j++) tg[j] = q.targets[j];
+    uint8_t **ptrs = reinterpret_cast<uint8_t **>(h + cb + tb);
+    for (size_t i = 0; i < n; i++) ptrs[i] = rows + i * r.row_len;
+    RSB_TRY(upload(s, q, st));
+    const uint64_t before = g_launches.load();
+    RSB_TRY(fft16_decode_run(dd, reinterpret_cast<const uint16_t *>(u), d, q.dev.bytes,
+                             reinterpret_cast<uint8_t *const *>(u + cb + tb), reinterpret_cast<const uint32_t *>(u + cb),
+                             e, r.row_len, st));
+    g.launches += g_launches.load() - before;
+    return stage_out(s, q, st);
   } else {
     if (e == 0) return RS_OK;
     uint16_t *nodes = reinterpret_cast<uint16_t *>(h), *tg = reinterpret_cast<uint16_t *>(h + up256(k * 2));
@@ -904,6 +933,19 @@ int rs_server_submit(rs_server_t *s, const rs_request *reqs, size_t n, int *stat
                             up256(fft16_table_bytes(*p));
           fits = fits || (need_fft <= s->cfg.arena_bytes && up256(q->up_bytes) <= s->cfg.pinned_bytes);
           q->fft16.reset();
+        }
+      }
+      if (r.field == 16 && r.op != RS_BATCH_ENCODE && !q->targets.empty()) {
+        auto dd = std::make_shared<Fft16Decode>();
+        if (fft16_decode_build(r.data_shards, r.parity_shards, q->surv, q->targets, *dd) &&
+            fft16_decode_preferred(*dd, r.data_shards)) {
+          q->dec_candidate = dd;
+          q->dec = dd;
+          q->scratch_budget = std::min<size_t>(kFft16ScratchBudget, s->cfg.arena_bytes / 8);
+          size_request(*q, false);
+          size_t need_dec = up256(payload_bytes(r)) + up256(q->up_bytes) + up256(q->dev_bytes);
+          fits = fits || (need_dec <= s->cfg.arena_bytes && up256(q->up_bytes) <= s->cfg.pinned_bytes);
+          q->dec.reset();
         }
       }
       if (!fits) st = RS_ERR_TOO_LARGE;
