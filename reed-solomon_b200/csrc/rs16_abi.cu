@@ -55,10 +55,10 @@ static int fft16_encode(const Gen16 &g, const uint8_t *in_base, uint64_t in_row,
                         uint8_t *const *d_ptrs, cudaStream_t st) {
   const size_t bytes = fft16_scratch_bytes(*g.fft, n_stripes, len, kFft16ScratchBudget);
   uint8_t *scratch = nullptr;
-  RSB_CU(cudaMallocAsync(&scratch, bytes, st));
+  RSB_CU(scratch_alloc(reinterpret_cast<void **>(&scratch), bytes, st));
   int rc = fft16_run(*g.fft, g.d_fft_cols, scratch, bytes, in_base, in_row, in_stripe, out_base, out_row, out_stripe,
                      d_ptrs, n_stripes, len, st);
-  cudaFreeAsync(scratch, st);
+  scratch_free(scratch, st);
   return rc;
 }
 
@@ -198,7 +198,7 @@ static int apply16_ptrs(const uint32_t *coeffs, uint32_t k, uint32_t rows, const
   for (uint32_t i = 0; i < k; i++) table[i] = in_ptrs[i];
   for (uint32_t j = 0; j < rows; j++) table[k + j] = out_ptrs[j];
   void *d_table = nullptr;
-  RSB_CU(cudaMallocAsync(&d_table, table.size() * sizeof(void *), st));
+  RSB_CU(scratch_alloc(&d_table, table.size() * sizeof(void *), st));
   RSB_CU(cudaMemcpyAsync(d_table, table.data(), table.size() * sizeof(void *), cudaMemcpyHostToDevice, st));
   Apply16Args a{};
   a.in_ptrs = reinterpret_cast<const uint8_t *const *>(d_table);
@@ -210,7 +210,7 @@ static int apply16_ptrs(const uint32_t *coeffs, uint32_t k, uint32_t rows, const
   a.n_stripes = 1;
   a.mismatch = mismatch;
   int st_ = launch_gf16(a, verify, st);
-  cudaFreeAsync(d_table, st);
+  scratch_free(d_table, st);
   return st_;
 }
 
@@ -229,13 +229,13 @@ static int fft16_reconstruct(const Gen16 &g, const Plan &plan, Exec &ex, uint8_t
   if (dev) {
     uint8_t *mem = nullptr;
     const size_t tbytes = (n * sizeof(void *) + 255) & ~size_t(255);
-    RSB_CU(cudaMallocAsync(&mem, tbytes + sbytes, st));
+    RSB_CU(scratch_alloc(reinterpret_cast<void **>(&mem), tbytes + sbytes, st));
     int rc = RS_OK;
     if (cudaMemcpyAsync(mem, shards, n * sizeof(void *), cudaMemcpyHostToDevice, st) != cudaSuccess) rc = RS_ERR_CUDA;
     if (rc == RS_OK)
       rc = fft16_decode_run(d, d_cols, mem + tbytes, sbytes, reinterpret_cast<uint8_t *const *>(mem), d_targets,
                             rows, len, st);
-    cudaFreeAsync(mem, st);
+    scratch_free(mem, st);
     return rc;
   }
   std::lock_guard<std::mutex> lock(ex.mu);
@@ -562,10 +562,10 @@ int rs16_encode_dev(rs16_t *c, uint8_t *const *d_shards, size_t n_shards, size_t
   cudaStream_t st = (cudaStream_t)stream;
   if (use_fft16(c)) {
     void *d_table = nullptr;
-    RSB_CU(cudaMallocAsync(&d_table, n * sizeof(void *), st));
+    RSB_CU(scratch_alloc(&d_table, n * sizeof(void *), st));
     RSB_CU(cudaMemcpyAsync(d_table, d_shards, n * sizeof(void *), cudaMemcpyHostToDevice, st));
     int rc = fft16_encode(g, nullptr, 0, 0, nullptr, 0, 0, 1, len, reinterpret_cast<uint8_t *const *>(d_table), st);
-    cudaFreeAsync(d_table, st);
+    scratch_free(d_table, st);
     return rc;
   }
   return apply16_ptrs(g.d_split, (uint32_t)g.k, (uint32_t)g.m, d_shards, d_shards + g.k, len, false, nullptr, st);

@@ -37,6 +37,32 @@ int ensure_device(int *device_out) {
   return RS_OK;
 }
 
+cudaError_t scratch_alloc(void **p, size_t bytes, cudaStream_t st) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaMallocAsync(p, bytes, st);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[dev]) {
+      cudaMemPoolProps props{};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      e = cudaMemPoolCreate(&pools[dev], &props);
+      if (e != cudaSuccess) {
+        pools[dev] = nullptr;
+        return e;
+      }
+      uint64_t keep = 1ull << 30;
+      cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
+  return cudaMallocFromPoolAsync(p, bytes, pools[dev], st);
+}
+
 Gf16Tables::Gf16Tables() : log(65536, 0), exp(2 * 65535, 0) {
   // Smallest element of full order 65535 = 3 * 5 * 17 * 257.
   auto power = [](uint16_t b, uint32_t e) {

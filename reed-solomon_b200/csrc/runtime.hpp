@@ -37,6 +37,14 @@ int ensure_device(int *device_out);
     if (st_ != RS_OK) return st_; \
   } while (0)
 
+// Stream-ordered scratch from a pool this library owns on the current device. The pool
+// keeps up to 1 GiB mapped between calls (the default pool returns memory at every
+// synchronisation, so large per-call scratch would be mapped again on each call).
+cudaError_t scratch_alloc(void **p, size_t bytes, cudaStream_t st);
+inline void scratch_free(void *p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
+
 // Grow-only device allocation owned by one execution context.
 struct DeviceBuf {
   uint8_t *ptr = nullptr;

