@@ -56,6 +56,7 @@ def parse():
                     help="workloads the tuner times (about 5 applicable configurations each)")
     ap.add_argument("--requests", type=int, default=400, help="requests of the serve workload")
     ap.add_argument("--rs16", default=None, help="rs16 workload: one shape K,M,STRIPES instead of both")
+    ap.add_argument("--mixed-stripes", type=int, default=10000, help="stripes of the mixed workload")
     return ap.parse_args()
 
 
@@ -318,7 +319,7 @@ def run_workload(args):
             line = {"metric": "RS(k,k) encode/reconstruct GB/s, 4096 stripes per launch", "unit": "GB/s",
                     "results": res}
         elif args.workload == "mixed":
-            res = workloads.mixed_batch()
+            res = workloads.mixed_batch(n=args.mixed_stripes)
             line = {"metric": "mixed-shape batch GB/s, batched+tuned vs plain", "unit": "GB/s",
                     "value": res["batched_gbs"], "results": res}
         elif args.workload == "rs16":
