@@ -240,15 +240,8 @@ int fft16_decode_run(const Fft16Decode &d, const uint16_t *d_cols, uint8_t *scra
       a.G = gn;
       a.n_stripes = 1;
       a.inverse = inverse;
-      const uint64_t tasks = (gn + 31) / 32;
-      const unsigned threads = (unsigned)(32 * std::min<uint64_t>(8, tasks));
-      const unsigned gy = (unsigned)std::min<uint64_t>(65535, (tasks * 32 + threads - 1) / threads);
-      if (lv == 2)
-        fft16_pass_kernel<2><<<dim3(N / 4, gy), threads, 0, st>>>(a);
-      else
-        fft16_pass_kernel<1><<<dim3(N / 2, gy), threads, 0, st>>>(a);
       g_launches++;
-      RSB_CU(cudaGetLastError());
+      RSB_CU(launch_fft16_pass(a, lv, st));
       return RS_OK;
     };
     const int lg = (int)d.lg;
@@ -328,15 +321,8 @@ int fft16_run(const Fft16Program &p, const uint16_t *d_cols, uint8_t *scratch, s
         a.G = gn;
         a.n_stripes = ns;
         a.inverse = s.inverse;
-        const uint64_t tasks = (uint64_t)ns * ((gn + 31) / 32);
-        const unsigned threads = (unsigned)(32 * std::min<uint64_t>(8, tasks));
-        const unsigned gy = (unsigned)std::min<uint64_t>(65535, (tasks * 32 + threads - 1) / threads);
-        if (lv == 2)
-          fft16_pass_kernel<2><<<dim3(s.size / 4, gy), threads, 0, st>>>(a);
-        else
-          fft16_pass_kernel<1><<<dim3(s.size / 2, gy), threads, 0, st>>>(a);
         g_launches++;
-        RSB_CU(cudaGetLastError());
+        RSB_CU(launch_fft16_pass(a, lv, st));
         return RS_OK;
       };
       // Levels of a transform: inverse 0, 1 | 2, 3 | ... (an odd top level alone, last);

@@ -101,67 +101,108 @@ __device__ __forceinline__ void store_reg16(uint32_t *p, const Reg16 &r) {
 
 // LV = 1: registers {i0, i0+h} at level L (h = 2^L). LV = 2: {i0, i0+h, i0+2h, i0+3h},
 // levels L and L+1 (inverse: L then L+1; forward: L+1 then L).
+//
+// One warp per CTA, persistent over items (butterfly group, task): item = group * tasks
+// + task, a task being one stripe's 32 symbol groups (one per lane). While an item is
+// computed, the next item's registers are already being copied into shared memory with
+// cp.async, so scratch loads overlap the multiplies; the item's three constants are
+// expanded into masks in shared memory (broadcast reads).
 template <int LV>
-__global__ void __launch_bounds__(kFft16Threads, 2) fft16_pass_kernel(const Fft16PassArgs a) {
-  constexpr int NC = LV == 2 ? 3 : 1;
+__global__ void __launch_bounds__(32, 16) fft16_pass_kernel(const Fft16PassArgs a) {
+  constexpr int NC = LV == 2 ? 3 : 1, NR = 1 << LV;
   __shared__ __align__(16) uint32_t mk[NC][256];
-  const uint32_t R = a.R, L = a.level, h = 1u << L;
-  const uint32_t grp = blockIdx.x;
-  const uint32_t blk = grp >> L, i = grp & (h - 1);
-  const uint32_t i0 = blk * (h << LV) + i;
-  uint32_t cidx[NC];
-  if constexpr (LV == 2) {
-    cidx[0] = R - (R >> L) + 2 * blk;          // level L, block of i0 / i0+h
-    cidx[1] = R - (R >> L) + 2 * blk + 1;      // level L, block of i0+2h / i0+3h
-    cidx[2] = R - (R >> (L + 1)) + blk;        // level L+1
-  } else {
-    cidx[0] = R - (R >> L) + blk;
-  }
-  for (uint32_t t = threadIdx.x; t < NC * 256; t += blockDim.x) {
-    const uint32_t c = t >> 8, b = (t >> 4) & 15, p = t & 15;
-    mk[c][t & 255] = ((a.cols[16 * cidx[c] + p] >> b) & 1) ? ~0u : 0u;
-  }
-  __syncthreads();
-  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
-  const uint64_t chunks = (a.G + 31) / 32;
-  const uint64_t tasks = (uint64_t)a.n_stripes * chunks;
-  for (uint64_t task = (uint64_t)blockIdx.y * warps + warp; task < tasks; task += (uint64_t)gridDim.y * warps) {
-    const uint64_t s = task / chunks;
-    const uint64_t g = (task % chunks) * 32 + lane;
-    if (g >= a.G) continue;
-    const uint64_t sb = s * a.src_regs + a.src_start, db = s * a.dst_regs + a.dst_start;
-    auto sw = [&](uint32_t r) { return ((sb + r) * a.G + g) * 16; };
-    auto dw = [&](uint32_t r) { return ((db + r) * a.G + g) * 16; };
-    if constexpr (LV == 2) {
-      Reg16 r0, r1, r2, r3;
-      load_reg16(a.src + sw(i0), r0);
-      load_reg16(a.src + sw(i0 + h), r1);
-      load_reg16(a.src + sw(i0 + 2 * h), r2);
-      load_reg16(a.src + sw(i0 + 3 * h), r3);
-      if (a.inverse) {
-        bfly16(r0, r1, mk[0], true);
-        bfly16(r2, r3, mk[1], true);
-        bfly16(r0, r2, mk[2], true);
-        bfly16(r1, r3, mk[2], true);
-      } else {
-        bfly16(r0, r2, mk[2], false);
-        bfly16(r1, r3, mk[2], false);
-        bfly16(r0, r1, mk[0], false);
-        bfly16(r2, r3, mk[1], false);
+  __shared__ __align__(16) uint4 stage[NR][4][32];  // [register][16-byte quarter][lane]
+  const uint32_t R = a.R, L = a.level, h = 1u << L, lane = threadIdx.x;
+  const uint32_t chunks = (uint32_t)((a.G + 31) / 32), tasks = a.n_stripes * chunks;
+  const uint32_t items = (R >> LV) * tasks;
+  struct Item {
+    uint32_t grp, s;
+    uint64_t g;
+  };
+  auto locate = [&](uint32_t item) {
+    Item it;
+    it.grp = item / tasks;
+    const uint32_t task = item - it.grp * tasks;
+    it.s = task / chunks;
+    it.g = (uint64_t)(task - it.s * chunks) * 32 + lane;
+    return it;
+  };
+  auto first_reg = [&](uint32_t grp) { return (grp >> L) * (h << LV) + (grp & (h - 1)); };
+  auto prefetch = [&](uint32_t item) {
+    const Item it = locate(item);
+    if (it.g < a.G) {
+      const uint32_t i0 = first_reg(it.grp);
+#pragma unroll
+      for (int q = 0; q < NR; q++) {
+        const uint32_t *p = a.src + (((uint64_t)it.s * a.src_regs + a.src_start + i0 + q * h) * a.G + it.g) * 16;
+#pragma unroll
+        for (int c = 0; c < 4; c++) cp_async16(&stage[q][c][lane], p + 4 * c);
       }
-      store_reg16(a.dst + dw(i0), r0);
-      store_reg16(a.dst + dw(i0 + h), r1);
-      store_reg16(a.dst + dw(i0 + 2 * h), r2);
-      store_reg16(a.dst + dw(i0 + 3 * h), r3);
-    } else {
-      Reg16 r0, r1;
-      load_reg16(a.src + sw(i0), r0);
-      load_reg16(a.src + sw(i0 + h), r1);
-      bfly16(r0, r1, mk[0], a.inverse != 0);
-      store_reg16(a.dst + dw(i0), r0);
-      store_reg16(a.dst + dw(i0 + h), r1);
     }
+    cp_async_commit();
+  };
+  uint32_t item = blockIdx.x;
+  if (item < items) prefetch(item);
+  for (; item < items; item += gridDim.x) {
+    const Item it = locate(item);
+    const uint32_t blk = it.grp >> L, i0 = first_reg(it.grp);
+    uint32_t cidx[NC];
+    if constexpr (LV == 2) {
+      cidx[0] = R - (R >> L) + 2 * blk;      // level L, block of i0 / i0+h
+      cidx[1] = R - (R >> L) + 2 * blk + 1;  // level L, block of i0+2h / i0+3h
+      cidx[2] = R - (R >> (L + 1)) + blk;    // level L+1
+    } else {
+      cidx[0] = R - (R >> L) + blk;
+    }
+    __syncwarp();  // the previous item's masks are no longer read
+    for (uint32_t t = lane; t < NC * 256; t += 32) {
+      const uint32_t c = t >> 8, b = (t >> 4) & 15, p = t & 15;
+      mk[c][t & 255] = ((a.cols[16 * cidx[c] + p] >> b) & 1) ? ~0u : 0u;
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    Reg16 r[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const uint4 v = stage[q][c][lane];
+        r[q][4 * c] = v.x, r[q][4 * c + 1] = v.y, r[q][4 * c + 2] = v.z, r[q][4 * c + 3] = v.w;
+      }
+    __syncwarp();  // the stage is read; the next item's copies may overwrite it
+    if (item + gridDim.x < items) prefetch(item + gridDim.x);
+    if (it.g >= a.G) continue;
+    if constexpr (LV == 2) {
+      if (a.inverse) {
+        bfly16(r[0], r[1], mk[0], true);
+        bfly16(r[2], r[3], mk[1], true);
+        bfly16(r[0], r[2], mk[2], true);
+        bfly16(r[1], r[3], mk[2], true);
+      } else {
+        bfly16(r[0], r[2], mk[2], false);
+        bfly16(r[1], r[3], mk[2], false);
+        bfly16(r[0], r[1], mk[0], false);
+        bfly16(r[2], r[3], mk[1], false);
+      }
+    } else {
+      bfly16(r[0], r[1], mk[0], a.inverse != 0);
+    }
+    const uint64_t db = (uint64_t)it.s * a.dst_regs + a.dst_start;
+#pragma unroll
+    for (int q = 0; q < NR; q++) store_reg16(a.dst + ((db + i0 + q * h) * a.G + it.g) * 16, r[q]);
   }
+}
+
+// Launch of a pass: one warp per CTA, up to 16 per SM, persistent over the items.
+inline cudaError_t launch_fft16_pass(const Fft16PassArgs &a, int lv, cudaStream_t st) {
+  const uint64_t tasks = (uint64_t)a.n_stripes * ((a.G + 31) / 32), items = ((uint64_t)a.R >> lv) * tasks;
+  if (items >= (1ull << 32)) return cudaErrorInvalidValue;
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)sm_count() * 16));
+  if (lv == 2)
+    fft16_pass_kernel<2><<<grid, 32, 0, st>>>(a);
+  else
+    fft16_pass_kernel<1><<<grid, 32, 0, st>>>(a);
+  return cudaGetLastError();
 }
 
 // Shard bytes -> bit planes: row r of stripe s (low plane [0,N), high plane [N,2N)),
