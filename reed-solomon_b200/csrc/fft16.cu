@@ -42,9 +42,20 @@ int log2_exact(uint64_t x) {
   return l;
 }
 
+// Table entry of a tower constant c (16 u16): the column bytes k_t * 2^p (p = 0..7) of
+// its Karatsuba factors k0 = c_lo, k1 = c_hi + c_lo, k2 = 32 c_hi, then 8 zero bytes.
+void push_const16(std::vector<uint16_t> &cols, uint16_t c) {
+  const uint8_t hi = (uint8_t)(c >> 8), lo = (uint8_t)c;
+  const uint8_t k[3] = {lo, (uint8_t)(hi ^ lo), gf8_mul(hi, 32)};
+  uint8_t bytes[32] = {};
+  for (int t = 0; t < 3; t++)
+    for (int q = 0; q < 8; q++) bytes[t * 8 + q] = gf8_mul(k[t], (uint8_t)(1u << q));
+  for (int w = 0; w < 16; w++) cols.push_back((uint16_t)(bytes[2 * w] | (bytes[2 * w + 1] << 8)));
+}
+
 uint64_t push_const(Fft16Program &p, uint16_t c) {
   uint64_t at = p.cols.size() / 16;
-  for (int b = 0; b < 16; b++) p.cols.push_back(gf16_mul(c, (uint16_t)(1u << b)));
+  push_const16(p.cols, c);
   return at;
 }
 
@@ -172,9 +183,7 @@ bool fft16_decode_build(size_t k, size_t m, const std::vector<uint32_t> &survivo
   for (uint32_t x = 0; x < N; x++) a[x] *= b[x];
   fwht(a);
   auto locator = [&](uint32_t x) { return T.exp[(a[x] / N) % 65535]; };
-  auto push16 = [&](uint16_t c) {
-    for (int p = 0; p < 16; p++) d.cols.push_back(gf16_mul(c, (uint16_t)(1u << p)));
-  };
+  auto push16 = [&](uint16_t c) { push_const16(d.cols, c); };
   // Transform constants (beta 0, both directions): (l, j) at N - (N >> l) + j.
   for (uint32_t l = 0; l < d.lg; l++)
     for (uint32_t j = 0; j < (N >> (l + 1)); j++) push16(what16()((int)l, (uint16_t)(j << (l + 1))));

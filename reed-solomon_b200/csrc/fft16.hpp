@@ -45,7 +45,7 @@ struct Fft16Program {
   uint32_t k = 0, m = 0, t = 0;
   std::vector<Fft16Step> interp;
   std::vector<Fft16Eval> evals;
-  std::vector<uint16_t> cols;  // 16 columns c * 2^p per constant
+  std::vector<uint16_t> cols;  // 16 u16 per constant: its Karatsuba factors' column bytes
   uint64_t butterflies = 0;    // per 32-symbol group (route estimate)
   bool uses_s = false;         // the interpolation needs S (k not a power of two)
   bool eval_in_place = false;  // a single evaluation runs on C itself (no W)

@@ -14,15 +14,19 @@
 // so bit p of a symbol's u16 value is plane p. Multiplying by a constant c is the
 // 16x16 GF(2) matrix whose column p is c * 2^p: plane b of the product is the XOR of
 // the planes p with bit b of c * 2^p set. The constants differ per butterfly block and
-// are only known at run time, so the matrix is applied as 256 masked XORs (one
-// three-input LOP3 each) with masks in shared memory.
+// are only known at run time, so the product is applied as masked XORs (one
+// three-input LOP3 each) with masks in shared memory, in the tower's Karatsuba form:
+// with c = (c_hi, c_lo) and x = (x_hi, x_lo), t0 = c_lo x_lo, t1 = (c_hi + c_lo)(x_lo +
+// x_hi), t2 = 32 c_hi x_hi, and c x = (t0 + t1) y + (t0 + t2) — three 8x8 GF(2)
+// matrices, 192 masks and ~216 LOP3 per product instead of a 16x16 matrix's 256.
+// A constant's table entry (16 u16) holds the column bytes k_t * 2^p of its three
+// GF(2^8) factors k0 = c_lo, k1 = c_hi + c_lo, k2 = 32 c_hi (24 bytes, 8 unused).
 //
 // Work split. The transform runs over a bitsliced scratch buffer, word
 // ((s * R + r) * G + g) * 16 + p for stripe s, register r of R, 32-symbol group g of G.
-// A pass applies one or two levels: a CTA (a multiple of 32 threads, at most 256) owns
-// one butterfly group (2 or 4 registers) and its warps take (stripe, 32 groups) tasks, one lane per 32-symbol group, so every
-// lane of a CTA uses the same constants and reads their masks as shared-memory
-// broadcasts.
+// A pass applies one or two levels. Its kernel runs one warp per CTA, persistent over
+// (butterfly group, stripe) items with one lane per 32-symbol group, so a warp's lanes
+// share the item's constants and read their masks as shared-memory broadcasts.
 #pragma once
 
 #include <cstdint>
@@ -39,7 +43,7 @@ constexpr int kFft16Threads = 256;
 struct Fft16PassArgs {
   const uint32_t *src;
   uint32_t *dst;
-  const uint16_t *cols;  // per constant: 16 columns c * 2^p; constant (l, j) at R - (R >> l) + j
+  const uint16_t *cols;  // 16 u16 per constant (see above); constant (l, j) at R - (R >> l) + j
   uint32_t R;            // registers in the transform (a power of two)
   uint32_t level;        // lowest level of the pass
   uint32_t src_regs, src_start, dst_regs, dst_start;
@@ -50,21 +54,61 @@ struct Fft16PassArgs {
 
 using Reg16 = uint32_t[16];
 
-// d ^= M * s, M as masks m[b * 16 + p] (all-ones when bit b of c * 2^p is set).
+constexpr uint32_t kMask16 = 192;  // masks per tower constant
+
+// Mask word t of a constant (layout [factor][output bit b][input bit p]): all-ones when
+// bit b of k_factor * 2^p is set.
+__device__ __forceinline__ uint32_t mask16(const uint16_t *cols, uint32_t t) {
+  const uint8_t byte = reinterpret_cast<const uint8_t *>(cols)[(t >> 6) * 8 + (t & 7)];
+  return ((byte >> ((t >> 3) & 7)) & 1) ? ~0u : 0u;
+}
+
+// Planes b of an 8x8 product of the 8 planes x, masks m[b * 8 + p], for output bit b.
+__device__ __forceinline__ uint32_t mat8_row(const uint32_t *x, const uint32_t *m, int b) {
+  const uint4 *m4 = reinterpret_cast<const uint4 *>(m + b * 8);
+  const uint4 u = m4[0], v = m4[1];
+  return (x[0] & u.x) ^ (x[1] & u.y) ^ (x[2] & u.z) ^ (x[3] & u.w) ^ (x[4] & v.x) ^ (x[5] & v.y) ^
+         (x[6] & v.z) ^ (x[7] & v.w);
+}
+
+// d ^= c * s in Karatsuba form (masks m: 3 x 64 words).
 __device__ __forceinline__ void mul16_acc(Reg16 &d, const Reg16 &s, const uint32_t *m) {
+  uint32_t lx[8], hx[8], sx[8];
 #pragma unroll
-  for (int b = 0; b < 16; b++) {
-    const uint4 *m4 = reinterpret_cast<const uint4 *>(m + b * 16);
-    uint32_t acc = d[b];
+  for (int p = 0; p < 8; p++) lx[p] = s[p], hx[p] = s[8 + p], sx[p] = s[p] ^ s[8 + p];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const uint4 v = m4[q];
-      acc ^= s[4 * q] & v.x;
-      acc ^= s[4 * q + 1] & v.y;
-      acc ^= s[4 * q + 2] & v.z;
-      acc ^= s[4 * q + 3] & v.w;
-    }
-    d[b] = acc;
+  for (int b = 0; b < 8; b++) {
+    const uint32_t t0 = mat8_row(lx, m, b), t1 = mat8_row(sx, m + 64, b), t2 = mat8_row(hx, m + 128, b);
+    d[b] ^= t0 ^ t2;
+    d[8 + b] ^= t0 ^ t1;
+  }
+}
+
+// d1 ^= c * s1 and d2 ^= c * s2 with one read of the masks.
+__device__ __forceinline__ void mul16_acc2(Reg16 &d1, const Reg16 &s1, Reg16 &d2, const Reg16 &s2,
+                                           const uint32_t *m) {
+  uint32_t l1[8], h1[8], x1[8], l2[8], h2[8], x2[8];
+#pragma unroll
+  for (int p = 0; p < 8; p++) {
+    l1[p] = s1[p], h1[p] = s1[8 + p], x1[p] = s1[p] ^ s1[8 + p];
+    l2[p] = s2[p], h2[p] = s2[8 + p], x2[p] = s2[p] ^ s2[8 + p];
+  }
+#pragma unroll
+  for (int b = 0; b < 8; b++) {
+    const uint4 *k0 = reinterpret_cast<const uint4 *>(m + b * 8);
+    const uint4 *k1 = reinterpret_cast<const uint4 *>(m + 64 + b * 8);
+    const uint4 *k2 = reinterpret_cast<const uint4 *>(m + 128 + b * 8);
+    const uint4 a0 = k0[0], a1 = k0[1], b0 = k1[0], b1 = k1[1], c0 = k2[0], c1 = k2[1];
+    auto row = [](const uint32_t *x, uint4 u, uint4 v) {
+      return (x[0] & u.x) ^ (x[1] & u.y) ^ (x[2] & u.z) ^ (x[3] & u.w) ^ (x[4] & v.x) ^ (x[5] & v.y) ^
+             (x[6] & v.z) ^ (x[7] & v.w);
+    };
+    const uint32_t t0 = row(l1, a0, a1), t1 = row(x1, b0, b1), t2 = row(h1, c0, c1);
+    d1[b] ^= t0 ^ t2;
+    d1[8 + b] ^= t0 ^ t1;
+    const uint32_t u0 = row(l2, a0, a1), u1 = row(x2, b0, b1), u2 = row(h2, c0, c1);
+    d2[b] ^= u0 ^ u2;
+    d2[8 + b] ^= u0 ^ u1;
   }
 }
 
@@ -81,6 +125,20 @@ __device__ __forceinline__ void bfly16(Reg16 &lo, Reg16 &hi, const uint32_t *m, 
   } else {
     mul16_acc(lo, hi, m);
     xor16(hi, lo);
+  }
+}
+
+// Two butterflies with the same constant: (lo1, hi1) and (lo2, hi2).
+__device__ __forceinline__ void bfly16x2(Reg16 &lo1, Reg16 &hi1, Reg16 &lo2, Reg16 &hi2, const uint32_t *m,
+                                         bool inverse) {
+  if (inverse) {
+    xor16(hi1, lo1);
+    xor16(hi2, lo2);
+    mul16_acc2(lo1, hi1, lo2, hi2, m);
+  } else {
+    mul16_acc2(lo1, hi1, lo2, hi2, m);
+    xor16(hi1, lo1);
+    xor16(hi2, lo2);
   }
 }
 
@@ -110,7 +168,7 @@ __device__ __forceinline__ void store_reg16(uint32_t *p, const Reg16 &r) {
 template <int LV>
 __global__ void __launch_bounds__(32, 16) fft16_pass_kernel(const Fft16PassArgs a) {
   constexpr int NC = LV == 2 ? 3 : 1, NR = 1 << LV;
-  __shared__ __align__(16) uint32_t mk[NC][256];
+  __shared__ __align__(16) uint32_t mk[NC][kMask16];
   __shared__ __align__(16) uint4 stage[NR][4][32];  // [register][16-byte quarter][lane]
   const uint32_t R = a.R, L = a.level, h = 1u << L, lane = threadIdx.x;
   const uint32_t chunks = (uint32_t)((a.G + 31) / 32), tasks = a.n_stripes * chunks;
@@ -155,9 +213,9 @@ __global__ void __launch_bounds__(32, 16) fft16_pass_kernel(const Fft16PassArgs 
       cidx[0] = R - (R >> L) + blk;
     }
     __syncwarp();  // the previous item's masks are no longer read
-    for (uint32_t t = lane; t < NC * 256; t += 32) {
-      const uint32_t c = t >> 8, b = (t >> 4) & 15, p = t & 15;
-      mk[c][t & 255] = ((a.cols[16 * cidx[c] + p] >> b) & 1) ? ~0u : 0u;
+    for (uint32_t t = lane; t < NC * kMask16; t += 32) {
+      const uint32_t c = t / kMask16, w = t - c * kMask16;
+      mk[c][w] = mask16(a.cols + 16 * cidx[c], w);
     }
     cp_async_wait_all();
     __syncwarp();
@@ -176,11 +234,9 @@ __global__ void __launch_bounds__(32, 16) fft16_pass_kernel(const Fft16PassArgs 
       if (a.inverse) {
         bfly16(r[0], r[1], mk[0], true);
         bfly16(r[2], r[3], mk[1], true);
-        bfly16(r[0], r[2], mk[2], true);
-        bfly16(r[1], r[3], mk[2], true);
+        bfly16x2(r[0], r[2], r[1], r[3], mk[2], true);
       } else {
-        bfly16(r[0], r[2], mk[2], false);
-        bfly16(r[1], r[3], mk[2], false);
+        bfly16x2(r[0], r[2], r[1], r[3], mk[2], false);
         bfly16(r[0], r[1], mk[0], false);
         bfly16(r[2], r[3], mk[1], false);
       }
@@ -263,9 +319,9 @@ __global__ void __launch_bounds__(kFft16Threads)
 __global__ void __launch_bounds__(kFft16Threads)
     fft16_mulxor_kernel(const uint32_t *src, uint32_t src_regs, uint32_t src_start, uint32_t *dst, uint32_t dst_regs,
                         uint32_t dst_start, uint32_t count, uint64_t G, uint32_t n_stripes, const uint16_t *cols) {
-  __shared__ __align__(16) uint32_t mk[256];
+  __shared__ __align__(16) uint32_t mk[kMask16];
   if (cols) {
-    for (uint32_t t = threadIdx.x; t < 256; t += blockDim.x) mk[t] = ((cols[t & 15] >> (t >> 4)) & 1) ? ~0u : 0u;
+    for (uint32_t t = threadIdx.x; t < kMask16; t += blockDim.x) mk[t] = mask16(cols, t);
     __syncthreads();
   }
   const uint64_t total = (uint64_t)n_stripes * count * G;
@@ -286,9 +342,9 @@ __global__ void __launch_bounds__(kFft16Threads)
 
 // ---- erasure decoding on the FFT route (one stripe, shards through a pointer table) ----
 //
-// Masks of one constant from its 16 columns into shared memory (all threads of the CTA).
+// Masks of one constant from its table entry into shared memory (all threads of the CTA).
 __device__ __forceinline__ void masks_from_cols(uint32_t *mk, const uint16_t *cols) {
-  for (uint32_t t = threadIdx.x; t < 256; t += blockDim.x) mk[t] = ((cols[t & 15] >> (t >> 4)) & 1) ? ~0u : 0u;
+  for (uint32_t t = threadIdx.x; t < kMask16; t += blockDim.x) mk[t] = mask16(cols, t);
 }
 
 // d = M * s (product only)
@@ -304,7 +360,7 @@ __device__ __forceinline__ void mul16_set(Reg16 &d, const Reg16 &s, const uint32
 __global__ void __launch_bounds__(kFft16Threads)
     fft16_scale_load_kernel(const uint8_t *const *ptrs, const uint16_t *cols, uint32_t n, uint64_t Nsym,
                             uint64_t g0, uint64_t G, uint32_t *dst) {
-  __shared__ __align__(16) uint32_t mk[256];
+  __shared__ __align__(16) uint32_t mk[kMask16];
   __shared__ int live;
   const uint32_t r = blockIdx.x;
   const uint16_t *c = cols + 16 * (uint64_t)r;
@@ -342,10 +398,12 @@ __global__ void __launch_bounds__(kFft16Threads)
 // constant derivative of the normalised subspace polynomial of level t.
 __global__ void __launch_bounds__(kFft16Threads)
     fft16_derivative_kernel(const uint32_t *src, uint32_t *dst, const uint16_t *kcols, uint32_t lg, uint64_t G) {
-  __shared__ __align__(16) uint32_t mk[16][256];
+  __shared__ __align__(16) uint32_t mk[16][kMask16];
   const uint32_t j = blockIdx.x;
-  for (uint32_t t = threadIdx.x; t < lg * 256; t += blockDim.x)
-    mk[t >> 8][t & 255] = ((kcols[16 * (t >> 8) + (t & 15)] >> ((t >> 4) & 15)) & 1) ? ~0u : 0u;
+  for (uint32_t t = threadIdx.x; t < lg * kMask16; t += blockDim.x) {
+    const uint32_t c = t / kMask16, w = t - c * kMask16;
+    mk[c][w] = mask16(kcols + 16 * c, w);
+  }
   __syncthreads();
   for (uint64_t g = threadIdx.x; g < G; g += blockDim.x) {
     Reg16 acc;
@@ -366,7 +424,7 @@ __global__ void __launch_bounds__(kFft16Threads)
 __global__ void __launch_bounds__(kFft16Threads)
     fft16_scale_store_kernel(const uint32_t *src, const uint32_t *rows, const uint16_t *tcols,
                              uint8_t *const *ptrs, uint64_t Nsym, uint64_t g0, uint64_t G) {
-  __shared__ __align__(16) uint32_t mk[256];
+  __shared__ __align__(16) uint32_t mk[kMask16];
   const uint32_t i = blockIdx.x, r = rows[i];
   masks_from_cols(mk, tcols + 16 * (uint64_t)i);
   __syncthreads();

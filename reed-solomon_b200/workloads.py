@@ -114,8 +114,11 @@ def mixed_batch(n=10000, seed=3, reps=5):
         S = int(math.exp(rng.uniform(math.log(1024), math.log(1 << 20))))
         op = RECONSTRUCT if rng.random() < 0.25 else ENCODE
         present = _erasures(rng, k + m, m) if op == RECONSTRUCT else None
-        specs.append((k, m, S, op, present, off))
-        off += ((k + m) * S + 255) & ~255
+        # Each shard starts on a 16-byte boundary, as separately allocated shard buffers
+        # do; its length S is any integer (most are not multiples of 16 or 64).
+        stride = (S + 15) & ~15
+        specs.append((k, m, S, stride, op, present, off))
+        off += ((k + m) * stride + 255) & ~255
     pool = torch.empty(off, dtype=torch.uint8, device="cuda")
     g = torch.Generator(device="cuda").manual_seed(seed)
     chunk = 1 << 30
@@ -123,9 +126,9 @@ def mixed_batch(n=10000, seed=3, reps=5):
         c1 = min(off, c0 + chunk)
         pool[c0:c1] = torch.randint(0, 256, (c1 - c0,), dtype=torch.uint8, device="cuda", generator=g)
     base = pool.data_ptr()
-    items = [(codecs[(k, m)], base + o, S, S, op, present) for k, m, S, op, present, o in specs]
+    items = [(codecs[(k, m)], base + o, st, S, op, present) for k, m, S, st, op, present, o in specs]
     nbytes = 0
-    for k, m, S, op, present, _ in specs:
+    for k, m, S, st, op, present, _ in specs:
         nbytes += (k + m) * S if op == ENCODE else (k + int((present == 0).sum())) * S
 
     t0 = time.perf_counter()
@@ -139,13 +142,30 @@ def mixed_batch(n=10000, seed=3, reps=5):
     for c in codecs.values():
         c.set_route("matrix")
 
+    # The single-stripe entry points through shard pointer tables, the tables built
+    # before timing (a caller holds its shard pointers already).
+    import ctypes
+
+    lib = _lib.load()
+    calls = []
+    for k, m, S, st, op, present, o in specs:
+        n_sh = k + m
+        ptrs = (ctypes.c_void_p * n_sh)(*[base + o + i * st for i in range(n_sh)])
+        h = codecs[(k, m)]._h
+        if op == ENCODE:
+            calls.append((lib.rs8_encode_dev, (h, ptrs, n_sh, S, 0), ptrs))
+        else:
+            lens = (ctypes.c_size_t * n_sh)(*([S] * n_sh))
+            flags = np.ascontiguousarray(present, np.uint8)
+            calls.append((lib.rs8_reconstruct_dev,
+                          (h, ptrs, lens, flags.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n_sh, 0, 0),
+                          (ptrs, lens, flags)))
+
     def plain():
-        for k, m, S, op, present, o in specs:
-            c = codecs[(k, m)]
-            if op == ENCODE:
-                c.encode_batch_dev(base + o, base + o + k * S, S, 1)
-            else:
-                c.reconstruct_batch_dev(base + o, 1, S, present)
+        for fn, args, _ in calls:
+            st = fn(*args)
+            if st:
+                raise RuntimeError("plain call status %d" % st)
 
     launches0 = _lib.load().rs_kernel_launch_count()
     t_plain = _time(plain, 1, warmup=1)
