@@ -60,6 +60,28 @@ def parse():
     return ap.parse_args()
 
 
+def rank_seed(rank):
+    """Each replica encodes its own stripes (weak scaling: no data is shared)."""
+    return 1234 + rank
+
+
+def max_over_ranks(ms, dist, device):
+    """The job's time: the slowest rank's (all ranks take part, then meet at a barrier)."""
+    if not dist:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    return float(t.item())
+
+
+def job_gbs(bytes_per_rank_step, world, ms_per_step):
+    """Whole-job algorithmic GB/s: every rank's bytes over the max-over-ranks step time."""
+    return bytes_per_rank_step * world / (ms_per_step * 1e-3) / 1e9
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -187,7 +209,7 @@ def run_ours(args, rank, world):
         import torch.distributed as dist
 
     S, L, k, m = args.stripes, SHARD, K_DATA, M_PARITY
-    g = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    g = torch.Generator(device="cuda").manual_seed(rank_seed(rank))
     data = torch.randint(0, 256, (S, k, L), dtype=torch.uint8, device="cuda", generator=g)
     parity = torch.empty((S, m, L), dtype=torch.uint8, device="cuda")
     rs = rsb.ReedSolomon(k, m)
@@ -226,13 +248,9 @@ def run_ours(args, rank, world):
     launches = rsb.kernel_launch_count() - launches0
     total_ms = t0.elapsed_time(t1)
     kern_ms = [a.elapsed_time(b) for a, b in ev]
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        dist.barrier()
+    total_ms = max_over_ranks(total_ms, dist, "cuda")
     ms_per_step = total_ms / args.steps
-    value = bytes_per_step * world / (ms_per_step * 1e-3) / 1e9
+    value = job_gbs(bytes_per_step, world, ms_per_step)
 
     # Plain: the matrix kernel, one stripe per launch.
     rs_plain = rsb.ReedSolomon(k, m)
