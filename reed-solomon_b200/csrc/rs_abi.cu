@@ -136,6 +136,11 @@ int launch_gf8(const ApplyArgs &a, const PtrTable *pt, bool verify, cudaStream_t
 // GF(2^8) codec
 // ------------------------------------------------------------------------------
 
+// Row pitch of device staging for host-pointer calls: whole 16-byte units, so every
+// staged shard starts aligned and the kernels' vector paths apply whatever the shard
+// length (a packed odd length would put most rows on the byte paths).
+static size_t pitch16(size_t len) { return (len + 15) & ~size_t(15); }
+
 // Encode route for a shape and length: the bitsliced FFT kernel where the shape has
 // a program and the shard holds at least one full 32-column group per thread pair,
 // else the matrix kernel.
@@ -261,17 +266,18 @@ static int reconstruct8(const Gen8 &g, PlanCache *cache, const Plan *fixed, Exec
   }
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
-  RSB_TRY(ex.buf.ensure((g.k + rows) * len));
+  const size_t pitch = pitch16(len);
+  RSB_TRY(ex.buf.ensure((g.k + rows) * pitch));
   for (size_t t = 0; t < g.k; t++)
-    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + t * len, shards[plan->survivors[t]], len,
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + t * pitch, shards[plan->survivors[t]], len,
                            cudaMemcpyHostToDevice, ex.stream));
   a.in_base = ex.buf.ptr;
-  a.in_row_stride = len;
-  a.out_base = ex.buf.ptr + g.k * len;
-  a.out_row_stride = len;
+  a.in_row_stride = pitch;
+  a.out_base = ex.buf.ptr + g.k * pitch;
+  a.out_row_stride = pitch;
   RSB_TRY(launch_gf8(a, nullptr, false, ex.stream));
   for (size_t j = 0; j < rows; j++)
-    RSB_CU(cudaMemcpyAsync(shards[outs[j]], ex.buf.ptr + (g.k + j) * len, len,
+    RSB_CU(cudaMemcpyAsync(shards[outs[j]], ex.buf.ptr + (g.k + j) * pitch, len,
                            cudaMemcpyDeviceToHost, ex.stream));
   RSB_CU(cudaStreamSynchronize(ex.stream));
   return RS_OK;
@@ -485,12 +491,13 @@ int rs8_encode(rs8_t *c, uint8_t *const *shards, size_t n_shards, size_t len) {
   Exec &ex = *c->exec;
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
-  RSB_TRY(ex.buf.ensure(n * len));
+  const size_t pitch = pitch16(len);
+  RSB_TRY(ex.buf.ensure(n * pitch));
   for (size_t i = 0; i < g.k; i++)
-    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * len, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
-  RSB_TRY(encode8_strided(c, ex.buf.ptr, len, 0, ex.buf.ptr + g.k * len, len, 0, 1, len, ex.stream));
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * pitch, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
+  RSB_TRY(encode8_strided(c, ex.buf.ptr, pitch, 0, ex.buf.ptr + g.k * pitch, pitch, 0, 1, len, ex.stream));
   for (size_t j = 0; j < g.m; j++)
-    RSB_CU(cudaMemcpyAsync(shards[g.k + j], ex.buf.ptr + (g.k + j) * len, len, cudaMemcpyDeviceToHost,
+    RSB_CU(cudaMemcpyAsync(shards[g.k + j], ex.buf.ptr + (g.k + j) * pitch, len, cudaMemcpyDeviceToHost,
                            ex.stream));
   RSB_CU(cudaStreamSynchronize(ex.stream));
   return RS_OK;
@@ -523,11 +530,12 @@ int rs8_encode_rows(rs8_t *c, const uint8_t *data, size_t data_len, size_t row_l
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
   size_t n = g.k + g.m;
-  RSB_TRY(ex.buf.ensure(n * row_len));
-  RSB_CU(cudaMemcpyAsync(ex.buf.ptr, data, data_len, cudaMemcpyHostToDevice, ex.stream));
-  RSB_TRY(encode8_strided(c, ex.buf.ptr, row_len, 0, ex.buf.ptr + data_len, row_len, 0, 1, row_len,
-                          ex.stream));
-  RSB_CU(cudaMemcpyAsync(parity, ex.buf.ptr + data_len, parity_len, cudaMemcpyDeviceToHost, ex.stream));
+  const size_t pitch = pitch16(row_len);
+  RSB_TRY(ex.buf.ensure(n * pitch));
+  uint8_t *d_par = ex.buf.ptr + g.k * pitch;
+  RSB_CU(cudaMemcpy2DAsync(ex.buf.ptr, pitch, data, row_len, row_len, g.k, cudaMemcpyHostToDevice, ex.stream));
+  RSB_TRY(encode8_strided(c, ex.buf.ptr, pitch, 0, d_par, pitch, 0, 1, row_len, ex.stream));
+  RSB_CU(cudaMemcpy2DAsync(parity, row_len, d_par, pitch, row_len, g.m, cudaMemcpyDeviceToHost, ex.stream));
   RSB_CU(cudaStreamSynchronize(ex.stream));
   return RS_OK;
 }
@@ -544,8 +552,10 @@ int rs8_encode_batch(rs8_t *c, const uint8_t *data, size_t data_stride, uint8_t 
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
   RSB_TRY(ex.pipe_streams());
+  // Device rows at a 16-byte pitch (pitched copies when row_len is not a multiple).
+  const size_t pitch = pitch16(row_len), ddin = g.k * pitch, ddout = g.m * pitch;
   // Chunks of about 64 MiB per slot, one slot per stream.
-  const size_t per = din + dout;
+  const size_t per = ddin + ddout;
   size_t chunk = std::max<size_t>(1, ((size_t)64 << 20) / per);
   chunk = std::min(chunk, n_stripes);
   RSB_TRY(ex.pipe_buf.ensure(Exec::kPipe * chunk * per));
@@ -554,20 +564,27 @@ int rs8_encode_batch(rs8_t *c, const uint8_t *data, size_t data_stride, uint8_t 
     const int slot = (int)(it % Exec::kPipe);
     cudaStream_t st = ex.pipe[slot];
     uint8_t *d_in = ex.pipe_buf.ptr + slot * chunk * per;
-    uint8_t *d_out = d_in + chunk * din;
-    if (data_stride == din) {
+    uint8_t *d_out = d_in + chunk * ddin;
+    if (pitch == row_len && data_stride == din) {
       RSB_CU(cudaMemcpyAsync(d_in, data + s0 * din, cnt * din, cudaMemcpyHostToDevice, st));
-    } else {
-      for (size_t s = 0; s < cnt; s++)
-        RSB_CU(cudaMemcpyAsync(d_in + s * din, data + (s0 + s) * data_stride, din, cudaMemcpyHostToDevice, st));
-    }
-    RSB_TRY(encode8_strided(c, d_in, row_len, din, d_out, row_len, dout, cnt, row_len, st));
-    if (parity_stride == dout) {
-      RSB_CU(cudaMemcpyAsync(parity + s0 * dout, d_out, cnt * dout, cudaMemcpyDeviceToHost, st));
-    } else {
-      for (size_t s = 0; s < cnt; s++)
-        RSB_CU(cudaMemcpyAsync(parity + (s0 + s) * parity_stride, d_out + s * dout, dout, cudaMemcpyDeviceToHost,
+    } else if (data_stride == din) {  // stripes back to back: one pitched copy of all rows
+      RSB_CU(cudaMemcpy2DAsync(d_in, pitch, data + s0 * din, row_len, row_len, cnt * g.k, cudaMemcpyHostToDevice,
                                st));
+    } else {
+      for (size_t s = 0; s < cnt; s++)
+        RSB_CU(cudaMemcpy2DAsync(d_in + s * ddin, pitch, data + (s0 + s) * data_stride, row_len, row_len, g.k,
+                                 cudaMemcpyHostToDevice, st));
+    }
+    RSB_TRY(encode8_strided(c, d_in, pitch, ddin, d_out, pitch, ddout, cnt, row_len, st));
+    if (pitch == row_len && parity_stride == dout) {
+      RSB_CU(cudaMemcpyAsync(parity + s0 * dout, d_out, cnt * dout, cudaMemcpyDeviceToHost, st));
+    } else if (parity_stride == dout) {
+      RSB_CU(cudaMemcpy2DAsync(parity + s0 * dout, row_len, d_out, pitch, row_len, cnt * g.m, cudaMemcpyDeviceToHost,
+                               st));
+    } else {
+      for (size_t s = 0; s < cnt; s++)
+        RSB_CU(cudaMemcpy2DAsync(parity + (s0 + s) * parity_stride, row_len, d_out + s * ddout, pitch, row_len, g.m,
+                                 cudaMemcpyDeviceToHost, st));
     }
   }
   for (auto st : ex.pipe) RSB_CU(cudaStreamSynchronize(st));
@@ -584,17 +601,18 @@ int rs8_verify(rs8_t *c, const uint8_t *const *shards, size_t n_shards, size_t l
   Exec &ex = *c->exec;
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
-  RSB_TRY(ex.buf.ensure(n * len));
+  const size_t pitch = pitch16(len);
+  RSB_TRY(ex.buf.ensure(n * pitch));
   RSB_TRY(ex.aux.ensure(64));
   for (size_t i = 0; i < n; i++)
-    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * len, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * pitch, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
   uint32_t *flag = reinterpret_cast<uint32_t *>(ex.aux.ptr);
   RSB_CU(cudaMemsetAsync(flag, 0, 4, ex.stream));
   ApplyArgs a{};
   a.in_base = ex.buf.ptr;
-  a.in_row_stride = len;
-  a.out_base = ex.buf.ptr + g.k * len;
-  a.out_row_stride = len;
+  a.in_row_stride = pitch;
+  a.out_base = ex.buf.ptr + g.k * pitch;
+  a.out_row_stride = pitch;
   a.coeffs = g.d_rows;
   a.k = (uint32_t)g.k;
   a.rows = (uint32_t)g.m;
