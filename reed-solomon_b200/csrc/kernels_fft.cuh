@@ -45,22 +45,79 @@ constexpr uint8_t gmul(uint8_t a, uint8_t b) {
   return r;
 }
 
-struct What {
-  uint8_t v[8][256];
+template <int K>
+constexpr int log2k() {
+  int l = 0;
+  while ((1 << l) < K) l++;
+  return l;
+}
+
+// Subspace basis of the transform. The parity values do not depend on how the additive
+// FFT enumerates V = {0 .. K-1}: for any ordered basis v_0 .. v_{n-1} of V, register i of
+// the inverse transform holds point P(i) = XOR of v_j over the bits j of i, and for any
+// beta in {K .. 2K-1} register i of the forward transform holds point beta ^ P(i). The
+// reference's programs use v_j = 2^j and beta = K; the bases below, found by
+// fft_basis_search.c, give butterfly constants with cheaper XOR networks (13% fewer
+// LOP3s in the constant multiplies at K = 32, 20% at K = 16). With lane groups of 2^W
+// lanes, v_0 .. v_{W-1} are single bits and the other vectors are clear of them, so a
+// lane's shard index is a compile-time part plus a per-lane part.
+struct FftBasis {
+  uint8_t v[8];
+  uint8_t beta;
 };
 
-// Normalised subspace polynomials: W_0(x) = x, W_{j+1}(x) = W_j(x) (W_j(x) + W_j(2^j)),
-// each level scaled so that its value at 2^j is 1.
-constexpr What make_what() {
+constexpr FftBasis fft_basis(int K, int W) {
+  switch (K) {
+    case 2: return {{1}, 2};
+    case 4: return {{2, 1}, 4};
+    case 8: return {{4, 2, 1}, 8};
+    case 16: return W == 1 ? FftBasis{{8, 3, 2, 4}, 16} : FftBasis{{4, 2, 9, 1}, 16};
+    case 32: return W == 1 ? FftBasis{{8, 19, 4, 6, 1}, 32} : FftBasis{{4, 2, 1, 8, 24}, 32};
+    case 64: return W == 2 ? FftBasis{{2, 4, 17, 41, 32, 16}, 68} : FftBasis{{2, 4, 1, 8, 40, 24}, 68};
+    default: return W == 3 ? FftBasis{{32, 64, 16, 3, 8, 4, 10}, 128} : FftBasis{{32, 16, 8, 64, 7, 3, 6}, 128};
+  }
+}
+
+// The basis spans {0 .. K-1}, its lane vectors are single bits, the rest avoid them, and
+// beta lies in {K .. 2K-1}.
+constexpr bool fft_basis_ok(int K, int W) {
+  const FftBasis b = fft_basis(K, W);
+  int n = 0, lanes = 0;
+  while ((1 << n) < K) n++;
+  bool seen[256] = {};
+  for (int i = 0; i < K; i++) {
+    int p = 0;
+    for (int j = 0; j < n; j++)
+      if ((i >> j) & 1) p ^= b.v[j];
+    if (p >= K || seen[p]) return false;
+    seen[p] = true;
+  }
+  for (int j = 0; j < W; j++) {
+    if (b.v[j] & (b.v[j] - 1)) return false;
+    lanes |= b.v[j];
+  }
+  for (int j = W; j < n; j++)
+    if (b.v[j] & lanes) return false;
+  return b.beta >= K && b.beta < 2 * K;
+}
+
+struct What {
+  uint8_t v[8][256];  // v[l][x]: normalised subspace polynomial of level l at x
+  uint8_t p[128];     // p[i] = P(i)
+};
+
+// W_0(x) = x, W_{j+1}(x) = W_j(x) (W_j(x) + W_j(v_j)), each level scaled so that its value
+// at v_j is 1.
+constexpr What make_what(FftBasis b, int n) {
   What w{};
   uint8_t raw[8][256] = {};
   for (int x = 0; x < 256; x++) raw[0][x] = (uint8_t)x;
-  for (int j = 0; j + 1 < 8; j++) {
-    uint8_t pivot = raw[j][1 << j];
+  for (int j = 0; j + 1 < n; j++) {
+    const uint8_t pivot = raw[j][b.v[j]];
     for (int x = 0; x < 256; x++) raw[j + 1][x] = gmul(raw[j][x], (uint8_t)(raw[j][x] ^ pivot));
   }
-  for (int j = 0; j < 8; j++) {
-    uint8_t pivot = raw[j][1 << j], inv = 0;
+  for (int j = 0; j < n; j++) {
+    uint8_t pivot = raw[j][b.v[j]], inv = 0;
     for (int c = 1; c < 256; c++)
       if (gmul(pivot, (uint8_t)c) == 1) {
         inv = (uint8_t)c;
@@ -68,10 +125,17 @@ constexpr What make_what() {
       }
     for (int x = 0; x < 256; x++) w.v[j][x] = gmul(raw[j][x], inv);
   }
+  for (int i = 0; i < (1 << n); i++) {
+    uint8_t p = 0;
+    for (int j = 0; j < n; j++)
+      if ((i >> j) & 1) p ^= b.v[j];
+    w.p[i] = p;
+  }
   return w;
 }
 
-inline constexpr What kWhat = make_what();
+template <int K, int W>
+inline constexpr What kWhat = make_what(fft_basis(K, W), log2k<K>());
 
 // Bit b of c * 2^bp: entry (b, bp) of the GF(2) matrix of multiply-by-c.
 constexpr bool mbit(uint8_t c, int b, int bp) { return (gmul(c, (uint8_t)(1u << bp)) >> b) & 1; }
@@ -115,23 +179,58 @@ __device__ __forceinline__ void xor_into(Reg &d, const Reg &s) {
   for (int b = 0; b < 8; b++) d[b] ^= s[b];
 }
 
+// Three-input XORs in d ^= C*s: ceil(n_b / 2) for output plane b with n_b terms.
+constexpr int mul_cost(uint8_t c) {
+  if (c <= 1) return c ? 8 : 0;
+  int n = 0;
+  for (int b = 0; b < 8; b++) {
+    int nb = 0;
+    for (int bp = 0; bp < 8; bp++) nb += mbit(c, b, bp);
+    n += (nb + 1) / 2;
+  }
+  return n;
+}
+
 // lo/hi butterfly with constant C; inverse: hi ^= lo, lo ^= C*hi; forward: lo ^= C*hi,
-// hi ^= lo (src/fft.rs:262-283).
+// hi ^= lo (src/fft.rs:262-283). The forward pair is also hi' = lo ^ (C+1)*hi, lo' =
+// hi' ^ hi, used when C+1 has the cheaper network (C = 1 then costs one register XOR).
 template <uint8_t C, bool INV>
 __device__ __forceinline__ void butterfly(Reg &lo, Reg &hi) {
-  if constexpr (INV) xor_into(hi, lo);
-  if constexpr (C == 1)
-    xor_into(lo, hi);
-  else if constexpr (C != 0)
-    mul_acc<C>(lo, hi);
-  if constexpr (!INV) xor_into(hi, lo);
+  if constexpr (INV) {
+    xor_into(hi, lo);
+    if constexpr (C == 1)
+      xor_into(lo, hi);
+    else if constexpr (C != 0)
+      mul_acc<C>(lo, hi);
+  } else if constexpr (C != 0 && mul_cost(C ^ 1) < mul_cost(C)) {
+    Reg t;
+#pragma unroll
+    for (int b = 0; b < 8; b++) t[b] = lo[b];
+    if constexpr ((C ^ 1) == 1)
+      xor_into(t, hi);
+    else if constexpr ((C ^ 1) != 0)
+      mul_acc<C ^ 1>(t, hi);
+    xor_into(hi, t);
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+      lo[b] = hi[b];
+      hi[b] = t[b];
+    }
+  } else {
+    if constexpr (C == 1)
+      xor_into(lo, hi);
+    else if constexpr (C != 0)
+      mul_acc<C>(lo, hi);
+    xor_into(hi, lo);
+  }
 }
 
 // Lane groups. A group of G = 2^W lanes shares one 32-column group; lane q holds
 // program registers i = (j << W) | q in its slots j = 0 .. K/G - 1.
 //
 // Level L >= W pairs slots j and j + 2^(L-W) within each lane; the butterfly's block
-// base has only bits >= W, so its constant is the same in every lane.
+// base has only bits >= W, so its constant WHAT_L(beta ^ P(base)) is the same in every
+// lane.
 template <int K, int W, int L, int BETA, bool INV>
 __device__ __forceinline__ void level_local(Reg (&r)[K >> W]) {
   constexpr int SJ = 1 << (L - W);  // slot stride
@@ -139,7 +238,7 @@ __device__ __forceinline__ void level_local(Reg (&r)[K >> W]) {
     constexpr int j = decltype(jj)::value;
     if constexpr (((j / SJ) & 1) == 0) {
       constexpr int base = (j << W) & ~((2 << L) - 1);
-      constexpr uint8_t c = kWhat.v[L][BETA ^ base];
+      constexpr uint8_t c = kWhat<K, W>.v[L][BETA ^ kWhat<K, W>.p[base]];
       butterfly<c, INV>(r[j], r[j + SJ]);
     }
   });
@@ -157,14 +256,14 @@ __device__ __forceinline__ void masked_mul_acc(Reg &d, const Reg &s, uint32_t ma
 }
 
 // The lane-dependent part of a cross-lane constant at level L. The block base of
-// register (j << W) | q is (j << W) | (q with bits <= L cleared); WHAT[L] is GF(2)-linear,
-// so the constant is WHAT[L][BETA ^ (j << W)] plus WHAT[L][2^t] for every lane bit t
-// in (L, W) that is set in q. qm[t] is all-ones when bit t of q is set.
-template <int W, int L, int T>
+// register (j << W) | q is (j << W) | (q with bits <= L cleared); P and WHAT_L are
+// GF(2)-linear, so the constant is WHAT_L(beta ^ P(j << W)) plus WHAT_L(v_t) for every
+// lane bit t in (L, W) that is set in q. qm[t] is all-ones when bit t of q is set.
+template <int K, int W, int L, int T>
 __device__ __forceinline__ void lane_terms(Reg &d, const Reg &s, const uint32_t (&qm)[8]) {
   if constexpr (T < W) {
-    masked_mul_acc<kWhat.v[L][1 << T]>(d, s, qm[T]);
-    lane_terms<W, L, T + 1>(d, s, qm);
+    masked_mul_acc<kWhat<K, W>.v[L][kWhat<K, W>.p[1 << T]]>(d, s, qm[T]);
+    lane_terms<K, W, L, T + 1>(d, s, qm);
   }
 }
 
@@ -177,7 +276,7 @@ __device__ __forceinline__ void level_cross(Reg (&r)[K >> W], uint32_t q, const 
   const uint32_t h1 = (q >> L) & 1, h0 = 1 - h1;
   static_for<0, (K >> W)>([&](auto jj) {
     constexpr int j = decltype(jj)::value;
-    constexpr uint8_t c = kWhat.v[L][BETA ^ (j << W)];
+    constexpr uint8_t c = kWhat<K, W>.v[L][BETA ^ kWhat<K, W>.p[j << W]];
     Reg p;
 #pragma unroll
     for (int b = 0; b < 8; b++) p[b] = __shfl_xor_sync(0xffffffffu, r[j][b], 1 << L);
@@ -193,7 +292,7 @@ __device__ __forceinline__ void level_cross(Reg (&r)[K >> W], uint32_t q, const 
         xor_into(v, t);
       else if constexpr (c != 0)
         mul_acc<c>(v, t);
-      lane_terms<W, L, L + 1>(v, t, qm);
+      lane_terms<K, W, L, L + 1>(v, t, qm);
 #pragma unroll
       for (int b = 0; b < 8; b++) r[j][b] = t[b] * h1 + v[b] * h0;
     } else {
@@ -210,7 +309,7 @@ __device__ __forceinline__ void level_cross(Reg (&r)[K >> W], uint32_t q, const 
 #pragma unroll
         for (int b = 0; b < 8; b++) u[b] = 0;
       }
-      lane_terms<W, L, L + 1>(u, z, qm);
+      lane_terms<K, W, L, L + 1>(u, z, qm);
 #pragma unroll
       for (int b = 0; b < 8; b++) r[j][b] ^= u[b] ^ (p[b] * h1);
     }
@@ -249,13 +348,6 @@ __device__ __forceinline__ void levels_down(Reg (&r)[K >> W], uint32_t q, const 
     level_any<K, W, L, BETA, false, SYNC>(r, q, qm);
     levels_down<K, W, L - 1, BETA, SYNC>(r, q, qm);
   }
-}
-
-template <int K>
-constexpr int log2k() {
-  int l = 0;
-  while ((1 << l) < K) l++;
-  return l;
 }
 
 }  // namespace fftc
@@ -451,11 +543,32 @@ __global__ void __launch_bounds__(THREADS, CTAS)
   using namespace fftc;
   using St = FftStage<THREADS>;
   constexpr int S = K >> W;  // slots per lane
+  constexpr int LG = log2k<K>();
+  static_assert(fft_basis_ok(K, W), "FFT basis");
+  constexpr FftBasis kB = fft_basis(K, W);
   const uint32_t tid = threadIdx.x;
   const uint32_t q = tid & ((1u << W) - 1);
   uint32_t qm[8];
 #pragma unroll
   for (int t = 0; t < 8; t++) qm[t] = ((q >> t) & 1) ? 0xffffffffu : 0u;
+  // Slot j holds register (j << W) | q: data shard P((j << W) | q) = P(j << W) + pq and
+  // parity shard beta ^ P(...) - K = ((beta ^ K ^ P(j << W)) & ~lane bits) + rq.
+  uint32_t pq = 0, lane_bits = 0;
+#pragma unroll
+  for (int t = 0; t < W; t++) {
+    pq |= (uint32_t)kB.v[t] & qm[t];
+    lane_bits |= kB.v[t];
+  }
+  const uint32_t rq = (((uint32_t)kB.beta ^ K) & lane_bits) ^ pq;
+  auto p_upper = [&](int j) -> uint32_t {  // P(j << W), folded for a compile-time j
+    uint32_t p = 0;
+#pragma unroll
+    for (int t = W; t < LG; t++)
+      if ((j >> (t - W)) & 1) p ^= kB.v[t];
+    return p;
+  };
+  auto in_index = [&](int j) -> uint32_t { return p_upper(j) + pq; };
+  auto out_index = [&](int j) -> uint32_t { return ((kB.beta ^ K ^ p_upper(j)) & ~lane_bits) + rq; };
   const uint64_t total = a.items ? a.total_groups : (uint64_t)a.n_stripes * a.groups_per_stripe;
   const uint64_t stride = (uint64_t)gridDim.x * (THREADS >> W);
   const uint64_t rounds = (total + stride - 1) / stride;
@@ -464,9 +577,9 @@ __global__ void __launch_bounds__(THREADS, CTAS)
 
   auto in_ptr = [&](const FftLoc &l, int j) -> const uint8_t * {
     if constexpr (PTRS)
-      return pt.in[(j << W) | q];
+      return pt.in[in_index(j)];
     else
-      return l.in0 + (uint64_t)((j << W) | q) * l.in_rs;
+      return l.in0 + (uint64_t)in_index(j) * l.in_rs;
   };
   // Whole 32-byte groups on 16-byte aligned rows (every group but a shard's last, for
   // aligned stripes) take the unrolled fast paths; the decision is made once per round.
@@ -523,20 +636,19 @@ __global__ void __launch_bounds__(THREADS, CTAS)
     }
     if (rd + 1 < rounds) prefetch(grp + stride);
     phase_sync<SYNC>();
-    constexpr int LG = log2k<K>();
-    // Interpolate: inverse transform on coset 0, levels 0 .. LG-1.
+    // Interpolate: inverse transform on V, levels 0 .. LG-1.
     levels_up<K, W, 0, 0, SYNC>(r, q, qm);
-    // Evaluate on coset K: forward transform, levels LG-1 .. 0.
-    levels_down<K, W, LG - 1, K, SYNC>(r, q, qm);
+    // Evaluate on the coset beta + V = {K .. 2K-1}: forward transform, levels LG-1 .. 0.
+    levels_down<K, W, LG - 1, kB.beta, SYNC>(r, q, qm);
     if (live) {
       const bool fast = whole(loc);
 #pragma unroll
       for (int j = 0; j < S; j++) {
         uint8_t *row;
         if constexpr (PTRS)
-          row = pt.out[(j << W) | q];
+          row = pt.out[out_index(j)];
         else
-          row = loc.out0 + (uint64_t)((j << W) | q) * loc.out_rs;
+          row = loc.out0 + (uint64_t)out_index(j) * loc.out_rs;
         uint32_t w[8];
 #pragma unroll
         for (int b = 0; b < 8; b++) w[b] = r[j][b];
