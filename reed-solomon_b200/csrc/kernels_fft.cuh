@@ -485,7 +485,7 @@ __device__ __forceinline__ FftLoc fft_locate(const FftArgs &a, uint64_t pair) {
 struct FftVariant {
   int threads, ctas, sync;
 };
-constexpr FftVariant kFftVariants[] = {{128, 3, 0}, {128, 4, 0}, {128, 2, 0}};
+constexpr FftVariant kFftVariants[] = {{128, 3, 0}, {128, 4, 0}, {128, 2, 0}, {256, 1, 0}};
 constexpr int kFftVariantCount = sizeof(kFftVariants) / sizeof(kFftVariants[0]);
 
 // Per-thread staging of one 32-column group in shared memory: shard slot j, half q
@@ -666,11 +666,12 @@ __global__ void __launch_bounds__(THREADS, CTAS)
   }
 }
 
-// Per-K launch shape (index into kFftVariants), defaults from a sweep on B200 (128
-// stripes of 1 MiB shards): K = 8 and 16 prefer 4 CTAs/SM, K = 32 and 64 two (their
-// 255-register ceiling removes spills), K = 128 three.
+// Per-K launch shape (index into kFftVariants), defaults from a sweep on B200 (16 GiB of
+// 1 MiB shards per launch): K = 4, 8 and 16 prefer four 128-thread CTAs per SM; K = 32, 64
+// and 128, whose slots need 255 registers, one 256-thread CTA per SM (10-12% above two
+// 128-thread CTAs with the same registers and staging).
 inline int &fft_variant_for(int K) {
-  static int v[8] = {0, 0, 0, 1, 1, 2, 2, 0};
+  static int v[8] = {0, 0, 1, 1, 1, 3, 3, 3};
   int l = 0;
   while ((1 << l) < K) l++;
   return v[l & 7];
@@ -704,7 +705,7 @@ constexpr int fft_w_hi(int K) { return K <= 8 ? 1 : K <= 32 ? 2 : K == 64 ? 3 : 
 
 // Selected lane-group width per K: 0 = fft_w_lo, 1 = fft_w_hi (rs_set_fft_lanes).
 inline int &fft_lanes_choice(int K) {
-  static int c[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // narrow groups measured fastest for every K
+  static int c[8] = {0, 0, 0, 0, 0, 0, 0, 1};  // narrow groups measured fastest but for K = 128
   int l = 0;
   while ((1 << l) < K) l++;
   return c[l & 7];
@@ -733,6 +734,7 @@ inline cudaError_t launch_fft_kw(const FftArgs &a, const PtrTableT<PTRS> &pt, cu
   } else {
     if (fft_variant_for(K) == 1) return launch_fft_kwv<K, W, PTRS, 1>(a, pt, st);
     if (fft_variant_for(K) == 2) return launch_fft_kwv<K, W, PTRS, 2>(a, pt, st);
+    if (fft_variant_for(K) == 3) return launch_fft_kwv<K, W, PTRS, 3>(a, pt, st);
     return launch_fft_kwv<K, W, PTRS, 0>(a, pt, st);
   }
 }

@@ -8,7 +8,8 @@ shapes, never arithmetic, so every choice yields the same bytes.
 
 Candidates (GF(2^8)):
   matrix route, tile variant 0..3 (parity rows per thread x output rows per CTA)
-  FFT route ((K,K) shapes), lane-group width narrow/wide x CTAs per SM 3/4/2
+  FFT route ((K,K) shapes), lane-group width narrow/wide x launch shape (threads x CTAs
+  per SM) 128x3 / 128x4 / 128x2 / 256x1
 """
 import ctypes
 import math
@@ -20,7 +21,7 @@ from .coder import ReedSolomon, _check
 
 CONFIGS = [("matrix", 0), ("matrix", 1), ("matrix", 2), ("matrix", 3),
            ("fft", (0, 0)), ("fft", (0, 1)), ("fft", (1, 0)), ("fft", (1, 1)),
-           ("fft", (0, 2)), ("fft", (1, 2))]
+           ("fft", (0, 2)), ("fft", (1, 2)), ("fft", (0, 3)), ("fft", (1, 3))]
 N_FEATURES = 5
 FFT_K = (2, 4, 8, 16, 32, 64, 128)
 
@@ -241,7 +242,7 @@ class CostModel:
         return P.argmin(axis=1)
 
 
-DEFAULT_FFT = {2: (0, 0), 4: (0, 0), 8: (0, 1), 16: (0, 1), 32: (0, 2), 64: (0, 2), 128: (0, 0)}
+DEFAULT_FFT = {2: (0, 0), 4: (0, 1), 8: (0, 1), 16: (0, 1), 32: (0, 3), 64: (0, 3), 128: (1, 3)}
 
 
 def default_choice(workloads, T):
