@@ -63,6 +63,22 @@ __device__ __forceinline__ uint32_t mask16(const uint16_t *cols, uint32_t t) {
   return ((byte >> ((t >> 3) & 7)) & 1) ? ~0u : 0u;
 }
 
+// All 192 masks of one constant, written by one warp: lane L owns the words w = L + 32 i
+// (i = 0 .. 5), whose input bit w & 7 = L & 7 is the same for all six, so it loads the
+// three column bytes f * 8 + (L & 7) once and takes bits (L >> 3) and (L >> 3) + 4 of each.
+__device__ __forceinline__ void masks_warp(uint32_t *m, const uint16_t *cols, uint32_t lane) {
+  const uint8_t *bytes = reinterpret_cast<const uint8_t *>(cols);
+  const uint32_t p = lane & 7, b = lane >> 3;
+  uint32_t v[3];
+#pragma unroll
+  for (int f = 0; f < 3; f++) v[f] = bytes[f * 8 + p];
+#pragma unroll
+  for (int f = 0; f < 3; f++) {
+    m[64 * f + lane] = ((v[f] >> b) & 1) ? ~0u : 0u;
+    m[64 * f + 32 + lane] = ((v[f] >> (b + 4)) & 1) ? ~0u : 0u;
+  }
+}
+
 // Planes b of an 8x8 product of the 8 planes x, masks m[b * 8 + p], for output bit b.
 __device__ __forceinline__ uint32_t mat8_row(const uint32_t *x, const uint32_t *m, int b) {
   const uint4 *m4 = reinterpret_cast<const uint4 *>(m + b * 8);
@@ -213,10 +229,8 @@ __global__ void __launch_bounds__(32, 16) fft16_pass_kernel(const Fft16PassArgs 
       cidx[0] = R - (R >> L) + blk;
     }
     __syncwarp();  // the previous item's masks are no longer read
-    for (uint32_t t = lane; t < NC * kMask16; t += 32) {
-      const uint32_t c = t / kMask16, w = t - c * kMask16;
-      mk[c][w] = mask16(a.cols + 16 * cidx[c], w);
-    }
+#pragma unroll
+    for (int c = 0; c < NC; c++) masks_warp(mk[c], a.cols + 16 * cidx[c], lane);
     cp_async_wait_all();
     __syncwarp();
     Reg16 r[NR];
