@@ -273,7 +273,8 @@ class ReedSolomon(_Coder):
         return self._L.rs8_encode_route(self._h, shard_len).decode()
 
     def set_route(self, route):
-        """0 = automatic, 1 = matrix kernel, 2 = bitsliced FFT kernel where one exists."""
+        """0 = automatic, 1 = matrix kernel, 2 = the shape's compiled bitsliced kernel (FFT or
+        generator) where one exists."""
         _check(self._L.rs8_set_route(self._h, {"auto": 0, "matrix": 1, "fft": 2}.get(route, route)))
 
     def encode_fused(self, shards):

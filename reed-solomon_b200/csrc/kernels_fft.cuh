@@ -687,13 +687,19 @@ inline int sm_count() {
   return n;
 }
 
-// Shapes with a bitsliced FFT kernel.
+// Shapes with a compiled bitsliced encode kernel: the FFT kernel for (K, K) with K a
+// power of two, the compile-time generator kernel (kernels_gen.cuh) for the reference's
+// other generated shapes and (20,12).
 struct FftShape {
   int k, m;
+  bool gen;  // generator kernel (no lane-group width or launch-shape choices)
 };
 
 inline const FftShape *find_fft_shape(size_t k, size_t m) {
-  static const FftShape shapes[] = {{2, 2}, {4, 4}, {8, 8}, {16, 16}, {32, 32}, {64, 64}, {128, 128}};
+  static const FftShape shapes[] = {{2, 2, false},   {4, 4, false},   {8, 8, false},  {16, 16, false},
+                                    {32, 32, false}, {64, 64, false}, {128, 128, false},
+                                    {7, 13, true},   {10, 10, true},  {14, 14, true}, {18, 6, true},
+                                    {20, 12, true}};
   for (const FftShape &s : shapes)
     if ((size_t)s.k == k && (size_t)s.m == m) return &s;
   return nullptr;
@@ -789,11 +795,24 @@ inline cudaError_t fft_launch_extern(const FftArgs &a, const PtrTableT<PTRS> &pt
   return cudaErrorInvalidValue;
 }
 
+// Generator-shape launchers (gen_k.cu).
+template <bool PTRS>
+cudaError_t gen8_launch(int k, int m, const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st);
+
 template <bool PTRS>
 inline int launch_fft_any(const FftShape &sh, const FftArgs &a, const PtrTableT<PTRS> &pt,
                           cudaStream_t st) {
   if (a.items ? a.total_groups == 0 : (a.len == 0 || a.n_stripes == 0)) return RS_OK;
   cudaError_t e;
+  if (sh.gen) {
+    e = gen8_launch<PTRS>(sh.k, sh.m, a, pt, st);
+    g_launches++;
+    if (e != cudaSuccess) {
+      set_cuda_error(e, "gen8_kernel launch");
+      return RS_ERR_CUDA;
+    }
+    return RS_OK;
+  }
   switch (sh.k) {
     case 2: e = fft_launch_extern<2, PTRS>(a, pt, st); break;
     case 4: e = fft_launch_extern<4, PTRS>(a, pt, st); break;

@@ -141,9 +141,9 @@ int launch_gf8(const ApplyArgs &a, const PtrTable *pt, bool verify, cudaStream_t
 // length (a packed odd length would put most rows on the byte paths).
 static size_t pitch16(size_t len) { return (len + 15) & ~size_t(15); }
 
-// Encode route for a shape and length: the bitsliced FFT kernel where the shape has
-// a program and the shard holds at least one full 32-column group per thread pair,
-// else the matrix kernel.
+// Encode route for a shape and length: the bitsliced FFT or generator kernel where the
+// shape has one and the shard holds at least two 32-column groups, else the matrix
+// kernel.
 bool use_fft8(const rs8_codec *c, size_t len) {
   int r = c->route.load();
   if (r == 1 || !c->gen->fft) return false;
@@ -334,7 +334,8 @@ int rs_device_check(void) { return ensure_device(nullptr); }
 uint64_t rs_kernel_launch_count(void) { return g_launches.load(); }
 
 int rs_set_fft_variant(size_t k, int variant) {
-  if (!find_fft_shape(k, k) || variant < 0 || variant >= kFftVariantCount) return -1;
+  const FftShape *sh = find_fft_shape(k, k);
+  if (!sh || sh->gen || variant < 0 || variant >= kFftVariantCount) return -1;
   int &v = fft_variant_for((int)k);
   int old = v;
   v = variant;
@@ -353,7 +354,8 @@ int rs_set_matrix_variant(int variant) {
 int rs_matrix_variant_count(void) { return kMatrixVariantCount; }
 
 int rs_set_fft_lanes(size_t k, int wide) {
-  if (!find_fft_shape(k, k) || wide < 0 || wide > 1) return -1;
+  const FftShape *sh = find_fft_shape(k, k);
+  if (!sh || sh->gen || wide < 0 || wide > 1) return -1;
   int &c = fft_lanes_choice((int)k);
   int old = c;
   c = wide;
@@ -472,7 +474,8 @@ int rs8_parity_matrix(const rs8_t *c, uint8_t *out, size_t out_len) {
 
 const char *rs8_encode_route(const rs8_t *c, size_t len) {
   if (!c) return "matrix";
-  return use_fft8(c, len) ? "fft-bitsliced" : "matrix";
+  if (!use_fft8(c, len)) return "matrix";
+  return c->gen->fft->gen ? "generator-bitsliced" : "fft-bitsliced";
 }
 
 int rs8_set_route(rs8_t *c, int route) {

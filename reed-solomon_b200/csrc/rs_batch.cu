@@ -97,7 +97,7 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     std::vector<uint32_t> surv, targets;
   };
   std::map<const Gen8 *, std::vector<Recon>> recon;  // per shape
-  std::map<int, std::vector<size_t>> fft_groups;     // K -> items
+  std::map<const FftShape *, std::vector<size_t>> fft_groups;  // compiled shape -> items
   std::vector<size_t> matrix_encodes;
 
   for (size_t i = 0; i < n_items; i++) {
@@ -124,7 +124,7 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     if (it.op == RS_BATCH_ENCODE) {
       b->bytes += n * it.row_len;
       if (!(flags & RS_BATCH_MATRIX_ONLY) && use_fft8(it.codec, it.row_len))
-        fft_groups[g.fft->k].push_back(i);
+        fft_groups[g.fft].push_back(i);
       else
         matrix_encodes.push_back(i);
       continue;
@@ -241,7 +241,7 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
   size_t ragged_off = ar.reserve(std::max<size_t>(ragged.size(), 1) * sizeof(RaggedItem));
   // ---- FFT items ----
   struct FftGroupOff {
-    int k;
+    const FftShape *shape;
     size_t off, n;
     uint64_t groups;
   };
@@ -254,7 +254,7 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
       const rs_batch_item &it = items[i];
       FftItem f{};
       f.in_base = it.d_rows;
-      f.out_base = it.d_rows + (size_t)kv.first * it.row_stride;
+      f.out_base = it.d_rows + (size_t)kv.first->k * it.row_stride;
       f.row_stride = it.row_stride;
       f.len = it.row_len;
       f.group_begin = g0;
@@ -310,7 +310,7 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
   RSB_CU(cudaStreamSynchronize(b->stream));
 
   for (auto &f : fgo)
-    b->ffts.push_back({find_fft_shape(f.k, f.k), reinterpret_cast<const FftItem *>(base + f.off), (uint32_t)f.n,
+    b->ffts.push_back({f.shape, reinterpret_cast<const FftItem *>(base + f.off), (uint32_t)f.n,
                        f.groups});
   b->ragged = reinterpret_cast<const RaggedItem *>(base + ragged_off);
   b->n_ragged = (uint32_t)ragged.size();

@@ -131,7 +131,7 @@ struct Req {
   std::vector<uint32_t> surv, targets;  // reconstruct: first k present; rebuilt rows
   uint64_t submit_ns = 0, admit_ns = 0, bytes = 0;
   int status = RS_OK;
-  bool fft = false;  // GF(2^8) (K,K) encode on the FFT kernel
+  bool fft = false;  // GF(2^8) encode on a compiled kernel (FFT or generator shape)
   // Working set, fixed when admitted.
   Span payload, up, dev, host;  // staged rows; uploaded descriptors; device-only; pinned image
   size_t up_bytes = 0, dev_bytes = 0;
@@ -509,8 +509,9 @@ static int enqueue_gf8(rs_server *s, Group &g, cudaStream_t st) {
     g.launches++;
     RSB_CU(cudaGetLastError());
   }
-  // Item arrays in the group's descriptor area: FFT items per K, then ragged items.
-  std::map<int, std::vector<FftItem>> ffts;
+  // Item arrays in the group's descriptor area: FFT / generator items per compiled
+  // shape, then ragged items.
+  std::map<const FftShape *, std::vector<FftItem>> ffts;
   std::vector<RaggedItem> ragged;
   uint32_t max_k = 1;
   uint64_t blocks = 0;
@@ -519,7 +520,7 @@ static int enqueue_gf8(rs_server *s, Group &g, cudaStream_t st) {
     const size_t k = q.r.data_shards, m = q.r.parity_shards, L = q.r.row_len;
     uint8_t *rows = rows_of(s, q);
     if (q.fft) {
-      auto &v = ffts[(int)k];
+      auto &v = ffts[find_fft_shape(k, m)];
       FftItem f{};
       f.in_base = rows;
       f.out_base = rows + k * L;
@@ -565,7 +566,7 @@ static int enqueue_gf8(rs_server *s, Group &g, cudaStream_t st) {
   for (auto &kv : ffts) {
     const auto &v = kv.second;
     uint64_t groups = v.back().group_begin + (v.back().len + 31) / 32;
-    RSB_TRY(launch_fft8_items(*find_fft_shape(kv.first, kv.first), reinterpret_cast<const FftItem *>(gd + off),
+    RSB_TRY(launch_fft8_items(*kv.first, reinterpret_cast<const FftItem *>(gd + off),
                               (uint32_t)v.size(), groups, st));
     g.launches++;
     off = up256(off + v.size() * sizeof(FftItem));
@@ -728,6 +729,7 @@ static void launch_group(rs_server *s, Group *g) {
 static bool route_fft(const rs_server *s, const rs_request &r) {
   const FftShape *sh = find_fft_shape(r.data_shards, r.parity_shards);
   if (!sh || r.op != RS_BATCH_ENCODE) return false;
+  if (sh->gen) return r.row_len >= 64;  // no per-size hints for generator shapes
   int kl = 0;
   while ((1 << (kl + 1)) <= sh->k) kl++;
   int bl = 0;
@@ -1003,7 +1005,7 @@ int rs_server_poll(rs_server_t *s, rs_completion *out, size_t cap, size_t *n_out
 int rs_server_set_fft_route(rs_server_t *s, size_t k, int log2_bytes, int route) {
   if (!s || route < 0 || route > 2 || log2_bytes < 0 || log2_bytes > 31) return RS_ERR_INVALID_ARGUMENT;
   const FftShape *sh = find_fft_shape(k, k);
-  if (!sh) return RS_ERR_INVALID_ARGUMENT;
+  if (!sh || sh->gen) return RS_ERR_INVALID_ARGUMENT;
   int kl = 0;
   while ((1 << (kl + 1)) <= sh->k) kl++;
   std::lock_guard<std::mutex> lock(s->mu);

@@ -10,6 +10,8 @@ Candidates (GF(2^8)):
   matrix route, tile variant 0..3 (parity rows per thread x output rows per CTA)
   FFT route ((K,K) shapes), lane-group width narrow/wide x launch shape (threads x CTAs
   per SM) 128x3 / 128x4 / 128x2 / 256x1
+  generator route (the compiled generator kernel of (7,13), (10,10), (14,14), (18,6),
+  (20,12))
 """
 import ctypes
 import math
@@ -21,9 +23,10 @@ from .coder import ReedSolomon, _check
 
 CONFIGS = [("matrix", 0), ("matrix", 1), ("matrix", 2), ("matrix", 3),
            ("fft", (0, 0)), ("fft", (0, 1)), ("fft", (1, 0)), ("fft", (1, 1)),
-           ("fft", (0, 2)), ("fft", (1, 2)), ("fft", (0, 3)), ("fft", (1, 3))]
+           ("fft", (0, 2)), ("fft", (1, 2)), ("fft", (0, 3)), ("fft", (1, 3)), ("gen", 0)]
 N_FEATURES = 5
 FFT_K = (2, 4, 8, 16, 32, 64, 128)
+GEN_SHAPES = ((7, 13), (10, 10), (14, 14), (18, 6), (20, 12))
 
 
 class Workload:
@@ -49,6 +52,8 @@ def applicable(w, cfg):
     route, _ = cfg
     if route == "fft":
         return w.erasures == 0 and w.k == w.m and w.k in FFT_K and w.shard_bytes >= 64
+    if route == "gen":
+        return w.erasures == 0 and (w.k, w.m) in GEN_SHAPES and w.shard_bytes >= 64
     return True
 
 
@@ -59,6 +64,8 @@ def apply_config(codec, w, cfg):
     if route == "matrix":
         codec.set_route("matrix")
         L.rs_set_matrix_variant(v)
+    elif route == "gen":
+        codec.set_route("fft")  # the shape's compiled kernel
     else:
         codec.set_route("fft")
         L.rs_set_fft_lanes(w.k, v[0])
@@ -137,9 +144,12 @@ def sample_workloads(n, seed, max_bytes=96 << 20):
     rng = np.random.default_rng(seed)
     out = []
     while len(out) < n:
-        if rng.random() < 0.4:
+        u = rng.random()
+        if u < 0.4:
             k = int(rng.choice([16, 32, 64, 128]))
             m = k
+        elif u < 0.5:
+            k, m = GEN_SHAPES[int(rng.integers(0, len(GEN_SHAPES)))]
         else:
             k = int(math.exp(rng.uniform(math.log(4), math.log(200))))
             m = int(rng.integers(2, min(3 * k, 256 - k) + 1)) if 256 - k >= 2 else 1
@@ -247,12 +257,14 @@ DEFAULT_FFT = {2: (0, 0), 4: (0, 1), 8: (0, 1), 16: (0, 1), 32: (0, 3), 64: (0, 
 
 def default_choice(workloads, T):
     """The method without the model: the library's default route and tile (the FFT
-    kernel with its per-K default launch shape where the shape has one, else matrix
-    tile 0)."""
+    kernel with its per-K default launch shape, or the generator kernel, where the
+    shape has one, else matrix tile 0)."""
     out = np.zeros(len(workloads), np.int64)
     for i, w in enumerate(workloads):
         if applicable(w, ("fft", (0, 0))) and np.isfinite(T[i, 4]):
             out[i] = CONFIGS.index(("fft", DEFAULT_FFT[w.k]))
+        elif applicable(w, ("gen", 0)):
+            out[i] = CONFIGS.index(("gen", 0))
     return out
 
 

@@ -165,7 +165,10 @@ def test_mul_slice_all_coefficients(gpu, O):
 
 def test_encode_route_introspection(gpu):
     assert gpu.ReedSolomon(32, 32).encode_route(1 << 20) == "fft-bitsliced"
-    assert gpu.ReedSolomon(20, 12).encode_route(1 << 20) == "matrix"
+    assert gpu.ReedSolomon(20, 12).encode_route(1 << 20) == "generator-bitsliced"
+    assert gpu.ReedSolomon(10, 10).encode_route(1 << 16) == "generator-bitsliced"
+    assert gpu.ReedSolomon(10, 10).encode_route(32) == "matrix"  # under two column groups
+    assert gpu.ReedSolomon(20, 10).encode_route(1 << 20) == "matrix"
 
 
 def test_clone_and_eq(gpu):
