@@ -57,6 +57,11 @@ def parse():
     ap.add_argument("--requests", type=int, default=400, help="requests of the serve workload")
     ap.add_argument("--rs16", default=None, help="rs16 workload: one shape K,M,STRIPES instead of both")
     ap.add_argument("--mixed-stripes", type=int, default=10000, help="stripes of the mixed workload")
+    ap.add_argument("--stripes-shapes", default=None,
+                    help="stripes workload: shapes K,M separated by '/' (default 32,32/16,16)")
+    ap.add_argument("--stripes-sizes", default=None,
+                    help="stripes workload: shard bytes separated by ',' (default 4096,65536,1048576)")
+    ap.add_argument("--stripes-count", type=int, default=4096, help="stripes workload: stripes per launch")
     return ap.parse_args()
 
 
@@ -333,9 +338,14 @@ def run_workload(args):
     launches0 = rsb.kernel_launch_count()
     with Clocks(0) as clk:
         if args.workload == "stripes":
-            res = workloads.stripes_sweep()
-            line = {"metric": "RS(k,k) encode/reconstruct GB/s, 4096 stripes per launch", "unit": "GB/s",
-                    "results": res}
+            kw = {"n_stripes": args.stripes_count}
+            if args.stripes_shapes:
+                kw["shapes"] = tuple(tuple(int(x) for x in sh.split(",")) for sh in args.stripes_shapes.split("/"))
+            if args.stripes_sizes:
+                kw["sizes"] = tuple(int(x) for x in args.stripes_sizes.split(","))
+            res = workloads.stripes_sweep(**kw)
+            line = {"metric": "RS(k,m) encode/reconstruct GB/s, %d stripes per launch" % args.stripes_count,
+                    "unit": "GB/s", "results": res}
         elif args.workload == "mixed":
             res = workloads.mixed_batch(n=args.mixed_stripes)
             line = {"metric": "mixed-shape batch GB/s, batched+tuned vs plain", "unit": "GB/s",

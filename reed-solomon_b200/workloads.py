@@ -77,6 +77,7 @@ def stripes_sweep(shapes=((32, 32), (16, 16)), sizes=(4096, 65536, 1 << 20), n_s
                 t = _time(enc, reps)
                 res["encode_%s_gbs" % route] = waves * wave * n * S / t / 1e9
             rs.set_route("auto")
+            res["encode_route"] = rs.encode_route(S)  # what the "fft" (compiled) timing ran
             rs.encode_batch_dev(rows, rows[:, k:], S, wave, data_stride=stride, parity_stride=stride)
             full = rows.clone()
             present = np.stack([_erasures(rng, n, m) for _ in range(wave)])
@@ -100,7 +101,8 @@ def stripes_sweep(shapes=((32, 32), (16, 16)), sizes=(4096, 65536, 1 << 20), n_s
 # ---- mixed batch: 10,000 stripes of nine shapes, 25% reconstruct ----
 
 def mixed_batch(n=10000, seed=3, reps=5):
-    """Batched+tuned (one graph: FFT per (K,K) shape + one ragged matrix launch) against
+    """Batched+tuned (one graph: one compiled-kernel launch per FFT or generator shape + one
+    ragged matrix launch) against
     the plain path (one matrix-kernel call per stripe; reconstructs build their decode
     rows per call), same stripes."""
     import torch

@@ -34,7 +34,7 @@ def encode_gpu(rs, data, m):
 
 
 SHAPES = [(7, 13), (10, 10), (20, 10), (4, 2), (6, 4), (17, 17), (32, 32), (16, 16), (14, 14),
-          (18, 6), (1, 1), (2, 2), (8, 8), (64, 64), (128, 128), (255, 1), (1, 255)]
+          (18, 6), (20, 12), (1, 1), (2, 2), (8, 8), (64, 64), (128, 128), (255, 1), (1, 255)]
 LENGTHS = [1, 15, 16, 17, 31, 32, 33, 63, 64, 65, 100, 987, 1024, 4103, 65536]
 
 
@@ -212,11 +212,12 @@ def test_encode_dev_pointers(gpu, O):
     assert rs.verify_dev(bufs, length)
 
 
-def test_encode_dev_unaligned_pointers(gpu, O):
-    """Shards at odd byte offsets take the FFT kernel's byte path; same bytes."""
+@pytest.mark.parametrize("k,m", [(16, 16), (10, 10)])
+def test_encode_dev_unaligned_pointers(gpu, O, k, m):
+    """Shards at odd byte offsets take the FFT / generator kernel's byte path; same bytes."""
     import torch
 
-    k, m, length = 16, 16, 4099
+    length = 4099
     rs = gpu.ReedSolomon(k, m)
     host = rand_data(k, length, 78)
     pool = torch.zeros((k + m) * (length + 64), dtype=torch.uint8, device="cuda")

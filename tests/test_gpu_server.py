@@ -54,7 +54,9 @@ PROBES = [
     (8, ENC, 32, 32, 4096, False),    # FFT K=32
     (8, ENC, 16, 16, 333, True),      # FFT K=16, ragged length, host staged
     (8, ENC, 128, 128, 2048, False),  # FFT K=128
-    (8, ENC, 10, 10, 1000, True),     # matrix (no FFT shape)
+    (8, ENC, 10, 10, 1000, True),     # generator kernel
+    (8, ENC, 20, 12, 4096, False),    # generator kernel, device rows
+    (8, ENC, 20, 10, 1000, True),     # matrix (no compiled shape)
     (8, REC, 20, 12, 777, False),
     (8, REC_DATA, 7, 13, 2048, True),
     (8, REC, 64, 64, 4100, False),
