@@ -9,8 +9,8 @@
 // planes, and plane b of parity j is then a fixed XOR network over the k x 8 data
 // planes (bit b of G[j][i] * 2^p selects plane p of shard i). With the constants known
 // at compile time that costs about 16 three-input XORs per coefficient on 32 columns,
-// a quarter of the matrix kernel's SWAR form (8 LOP3 per coefficient per 4 columns),
-// and at these sizes no more than the reference's FFT programs would.
+// a quarter of the matrix kernel's SWAR form (8 LOP3 per coefficient per 4 columns);
+// at k + m <= 32 an FFT program's butterflies would save little over that.
 #pragma once
 
 #include "kernels_fft.cuh"
