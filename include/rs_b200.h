@@ -191,8 +191,10 @@ size_t rs8_reconstruct_batch_noalloc_limit(size_t data_shards, size_t parity_sha
 /* ---- mixed batches: stripes of any GF(2^8) shapes, lengths and erasure patterns ----
  * No counterpart in the reference (it codes one stripe per call on one core). A batch
  * is validated and planned once: decode matrices for every reconstruct item are built
- * on the device in one launch per shape, the work is grouped by route (bitsliced FFT
- * per (K,K) shape, one ragged matrix launch for the rest) and captured into a CUDA
+ * on the device in one launch per shape, the work is grouped by route (one compiled
+ * bitsliced launch per FFT or generator shape, one ragged matrix launch for the rest;
+ * missing parity of reconstructs on compiled shapes is regenerated by a compiled launch
+ * that stores only the missing rows, after the data rows) and captured into a CUDA
  * graph; rs_batch_launch replays it. Each item's status is the reference error its
  * single-stripe call would return (0 = Ok); failed items are left out of the graph. */
 enum rs_batch_op {
@@ -217,8 +219,10 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
                     rs_batch_t **out);
 /* Enqueues one replay of the batch on `stream`. */
 int rs_batch_launch(rs_batch_t *batch, void *stream);
-/* Kernel launches per replay, stripes on each route, algorithmic bytes per replay
- * ((k+m)*len per encode, (k+e)*len per reconstruct rebuilding e rows). */
+/* Kernel launches per replay, stripes on each route (a stripe with any matrix work
+ * counts as a matrix item, one with compiled-kernel work only as an FFT item),
+ * algorithmic bytes per replay ((k+m)*len per encode, (k+e)*len per reconstruct
+ * rebuilding e rows). */
 int rs_batch_stats(const rs_batch_t *batch, size_t *launches, size_t *fft_items,
                    size_t *matrix_items, uint64_t *bytes);
 void rs_batch_free(rs_batch_t *batch);

@@ -431,7 +431,14 @@ struct FftArgs {
   uint64_t total_groups;
   // Pointer-table form: every shard pointer is 16-byte aligned (set by the host).
   int ptrs_aligned;
+  // Parity rows to store, 4 words (rows 0..127) per stripe, or per item in the ragged
+  // form; null stores every row. Reconstruct uses it to rebuild only the missing parity.
+  const uint32_t *store_mask;
 };
+
+__device__ __forceinline__ bool fft_store_row(const FftArgs &a, uint32_t unit, uint32_t row) {
+  return !a.store_mask || ((a.store_mask[4 * (uint64_t)unit + (row >> 5)] >> (row & 31)) & 1u);
+}
 
 // Where one lane pair's 32-column group lives.
 struct FftLoc {
@@ -439,6 +446,7 @@ struct FftLoc {
   uint8_t *out0;        // parity row 0
   uint64_t in_rs, out_rs;
   uint64_t col, remain;  // remain = 0 past the end
+  uint32_t unit;         // stripe (strided form) or item (ragged form)
 };
 
 __device__ __forceinline__ FftLoc fft_locate(const FftArgs &a, uint64_t pair) {
@@ -454,6 +462,7 @@ __device__ __forceinline__ FftLoc fft_locate(const FftArgs &a, uint64_t pair) {
         hi = mid;
     }
     const FftItem &it = a.items[lo];
+    l.unit = lo;
     l.in0 = it.in_base;
     l.out0 = it.out_base;
     l.in_rs = l.out_rs = it.row_stride;
@@ -471,6 +480,7 @@ __device__ __forceinline__ FftLoc fft_locate(const FftArgs &a, uint64_t pair) {
     s = (uint32_t)(pair / a.groups_per_stripe);
     g = (uint32_t)(pair - (uint64_t)s * a.groups_per_stripe);
   }
+  l.unit = s;
   l.in0 = a.in_base + s * a.in_stripe_stride;
   l.out0 = a.out_base + s * a.out_stripe_stride;
   l.in_rs = a.in_row_stride;
@@ -644,6 +654,7 @@ __global__ void __launch_bounds__(THREADS, CTAS)
       const bool fast = whole(loc);
 #pragma unroll
       for (int j = 0; j < S; j++) {
+        if (!fft_store_row(a, loc.unit, out_index(j))) continue;
         uint8_t *row;
         if constexpr (PTRS)
           row = pt.out[out_index(j)];
@@ -850,11 +861,12 @@ inline int launch_fft8(const FftShape &sh, const uint8_t *in_base, uint64_t in_r
 
 // Ragged batch of (K, K) stripes described by a device item array.
 inline int launch_fft8_items(const FftShape &sh, const FftItem *d_items, uint32_t n_items,
-                             uint64_t total_groups, cudaStream_t st) {
+                             uint64_t total_groups, cudaStream_t st, const uint32_t *store_mask = nullptr) {
   FftArgs a{};
   a.items = d_items;
   a.n_items = n_items;
   a.total_groups = total_groups;
+  a.store_mask = store_mask;
   PtrTableT<false> pt{};
   return launch_fft_any<false>(sh, a, pt, st);
 }

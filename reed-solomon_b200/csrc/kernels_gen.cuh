@@ -133,6 +133,7 @@ __global__ void __launch_bounds__(THREADS, CTAS)
     const bool fast = whole(loc);
     static_for<0, MP>([&](auto jj) {
       constexpr int j = decltype(jj)::value;
+      if (!fft_store_row(a, loc.unit, j)) return;
       Reg acc;
 #pragma unroll
       for (int b = 0; b < 8; b++) acc[b] = 0;

@@ -800,10 +800,19 @@ int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, s
   const Gen8 &g = *c->gen;
   const size_t k = g.k, n = g.k + g.m;
   cudaStream_t st = (cudaStream_t)stream;
+  // Where the shape has a compiled encode kernel, missing parity is regenerated by it
+  // from the data rows once they are whole, storing only the missing rows: the matrix
+  // route then applies (missing data) x k decode coefficients per column instead of
+  // (missing data + missing parity) x k. Measured on B200 (RS(32,32), 1..m erasures per
+  // stripe, both forms timed in one process): +10% at 4 KiB shards, +21% at 16 KiB,
+  // +28% at 64 KiB.
+  const bool split = !data_only && use_fft8(c, row_len);
   // Host side: per-stripe survivors and targets.
   std::vector<uint16_t> surv(n_stripes * k), targ(n_stripes * g.m), ntarg(n_stripes);
   std::vector<int> status(n_stripes, 0);
-  uint32_t max_rows = 1;
+  std::vector<FftItem> items;       // split: stripes with missing parity
+  std::vector<uint32_t> masks;      // split: 4 words of missing parity rows per item
+  uint32_t max_rows = 0;
   std::vector<uint32_t> s_surv, s_md, s_mp;
   size_t live = 0;
   for (size_t s = 0; s < n_stripes; s++) {
@@ -825,8 +834,19 @@ int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, s
     for (size_t t = 0; t < k; t++) surv[s * k + t] = (uint16_t)s_surv[t];
     size_t r = 0;
     for (uint32_t x : s_md) targ[s * g.m + r++] = (uint16_t)x;
-    if (!data_only)
+    if (split && !s_mp.empty()) {
+      FftItem f{};
+      f.in_base = d_rows + s * stripe_stride;
+      f.out_base = d_rows + s * stripe_stride + k * row_len;
+      f.row_stride = row_len;
+      f.len = row_len;
+      f.group_begin = items.empty() ? 0 : items.back().group_begin + (row_len + 31) / 32;
+      items.push_back(f);
+      masks.resize(masks.size() + 4, 0u);
+      for (uint32_t x : s_mp) masks[masks.size() - 4 + (x - k) / 32] |= 1u << ((x - k) % 32);
+    } else if (!data_only) {
       for (uint32_t x : s_mp) targ[s * g.m + r++] = (uint16_t)x;
+    }
     ntarg[s] = (uint16_t)r;
     max_rows = std::max<uint32_t>(max_rows, (uint32_t)r);
     live++;
@@ -837,50 +857,62 @@ int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, s
   Exec &ex = *c->exec;
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
-  // Device layout: surv | targ (max m per stripe) | ntarg | coeff rows | plan status.
+  // Device layout: surv | targ (max m per stripe) | ntarg | coeff rows | plan status |
+  // parity items | parity masks.
   size_t b_surv = surv.size() * 2, b_targ = targ.size() * 2, b_nt = ntarg.size() * 2;
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   size_t o_targ = al(b_surv), o_nt = o_targ + al(b_targ), o_rows = o_nt + al(b_nt);
   size_t b_rows = n_stripes * (size_t)g.m * k;
   size_t o_stat = o_rows + al(b_rows);
-  RSB_TRY(ex.aux.ensure(o_stat + al(n_stripes * sizeof(int))));
+  size_t o_items = o_stat + al(n_stripes * sizeof(int));
+  size_t o_masks = o_items + al(items.size() * sizeof(FftItem));
+  RSB_TRY(ex.aux.ensure(o_masks + al(masks.size() * sizeof(uint32_t))));
   uint8_t *base = ex.aux.ptr;
-  RSB_CU(cudaMemcpyAsync(base, surv.data(), b_surv, cudaMemcpyHostToDevice, st));
-  RSB_CU(cudaMemcpyAsync(base + o_targ, targ.data(), b_targ, cudaMemcpyHostToDevice, st));
-  RSB_CU(cudaMemcpyAsync(base + o_nt, ntarg.data(), b_nt, cudaMemcpyHostToDevice, st));
-  PlanArgs pa{};
-  pa.gen = g.d_rows;
-  pa.k = (uint32_t)k;
-  pa.m = (uint32_t)g.m;
-  pa.survivors = reinterpret_cast<uint16_t *>(base);
-  pa.targets = reinterpret_cast<uint16_t *>(base + o_targ);
-  pa.n_targets = reinterpret_cast<uint16_t *>(base + o_nt);
-  pa.max_rows = (uint32_t)g.m;
-  pa.out = base + o_rows;
-  pa.status = reinterpret_cast<int *>(base + o_stat);
-  size_t smem = plan_smem((uint32_t)k).total;
-  if (smem > 48 * 1024)
-    RSB_CU(cudaFuncSetAttribute(gf8_plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  gf8_plan_kernel<<<(unsigned)n_stripes, 256, smem, st>>>(pa);
-  g_launches++;
-  RSB_CU(cudaGetLastError());
-  ApplyArgs a{};
-  a.in_base = d_rows;
-  a.in_row_stride = row_len;
-  a.in_stripe_stride = stripe_stride;
-  a.out_base = d_rows;
-  a.out_row_stride = row_len;
-  a.out_stripe_stride = stripe_stride;
-  a.coeffs = base + o_rows;
-  a.coeff_stripe_stride = (uint64_t)g.m * k;
-  a.rows_per_stripe = pa.n_targets;
-  a.in_map = pa.survivors;
-  a.out_map = pa.targets;
-  a.k = (uint32_t)k;
-  a.rows = (uint32_t)g.m;
-  a.len = row_len;
-  a.n_stripes = (uint32_t)n_stripes;
-  return launch_gf8(a, nullptr, false, st);
+  if (max_rows > 0) {
+    RSB_CU(cudaMemcpyAsync(base, surv.data(), b_surv, cudaMemcpyHostToDevice, st));
+    RSB_CU(cudaMemcpyAsync(base + o_targ, targ.data(), b_targ, cudaMemcpyHostToDevice, st));
+    RSB_CU(cudaMemcpyAsync(base + o_nt, ntarg.data(), b_nt, cudaMemcpyHostToDevice, st));
+    PlanArgs pa{};
+    pa.gen = g.d_rows;
+    pa.k = (uint32_t)k;
+    pa.m = (uint32_t)g.m;
+    pa.survivors = reinterpret_cast<uint16_t *>(base);
+    pa.targets = reinterpret_cast<uint16_t *>(base + o_targ);
+    pa.n_targets = reinterpret_cast<uint16_t *>(base + o_nt);
+    pa.max_rows = (uint32_t)g.m;
+    pa.out = base + o_rows;
+    pa.status = reinterpret_cast<int *>(base + o_stat);
+    size_t smem = plan_smem((uint32_t)k).total;
+    if (smem > 48 * 1024)
+      RSB_CU(cudaFuncSetAttribute(gf8_plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    gf8_plan_kernel<<<(unsigned)n_stripes, 256, smem, st>>>(pa);
+    g_launches++;
+    RSB_CU(cudaGetLastError());
+    ApplyArgs a{};
+    a.in_base = d_rows;
+    a.in_row_stride = row_len;
+    a.in_stripe_stride = stripe_stride;
+    a.out_base = d_rows;
+    a.out_row_stride = row_len;
+    a.out_stripe_stride = stripe_stride;
+    a.coeffs = base + o_rows;
+    a.coeff_stripe_stride = (uint64_t)g.m * k;
+    a.rows_per_stripe = pa.n_targets;
+    a.in_map = pa.survivors;
+    a.out_map = pa.targets;
+    a.k = (uint32_t)k;
+    a.rows = (uint32_t)g.m;
+    a.len = row_len;
+    a.n_stripes = (uint32_t)n_stripes;
+    RSB_TRY(launch_gf8(a, nullptr, false, st));
+  }
+  if (items.empty()) return RS_OK;
+  RSB_CU(cudaMemcpyAsync(base + o_items, items.data(), items.size() * sizeof(FftItem), cudaMemcpyHostToDevice, st));
+  RSB_CU(cudaMemcpyAsync(base + o_masks, masks.data(), masks.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                         st));
+  const uint64_t groups = items.back().group_begin + (row_len + 31) / 32;
+  return launch_fft8_items(*g.fft, reinterpret_cast<const FftItem *>(base + o_items), (uint32_t)items.size(), groups,
+                           st, reinterpret_cast<const uint32_t *>(base + o_masks));
 }
 
 // ------------------------------- gf slices -----------------------------------

@@ -35,8 +35,10 @@ struct rs_batch {
     const FftItem *items;
     uint32_t n;
     uint64_t groups;
+    const uint32_t *masks;  // parity rows to store per item; null: every row
   };
-  std::vector<FftLaunch> ffts;
+  std::vector<FftLaunch> ffts;    // encodes
+  std::vector<FftLaunch> regens;  // missing parity of reconstructs, after the data rows
   const RaggedItem *ragged = nullptr;
   uint32_t n_ragged = 0;
   uint64_t ragged_blocks = 0;
@@ -60,6 +62,7 @@ static int batch_enqueue(rs_batch *b, cudaStream_t st) {
     g_launches++;
     RSB_CU(cudaGetLastError());
   }
+  for (const auto &f : b->regens) RSB_TRY(launch_fft8_items(*f.shape, f.items, f.n, f.groups, st, f.masks));
   return RS_OK;
 }
 
@@ -98,6 +101,12 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
   };
   std::map<const Gen8 *, std::vector<Recon>> recon;  // per shape
   std::map<const FftShape *, std::vector<size_t>> fft_groups;  // compiled shape -> items
+  struct Regen {
+    size_t item;
+    std::vector<uint32_t> parity;  // missing parity shard indexes
+    bool only;                     // no data rows to rebuild first
+  };
+  std::map<const FftShape *, std::vector<Regen>> regen_groups;
   std::vector<size_t> matrix_encodes;
 
   for (size_t i = 0; i < n_items; i++) {
@@ -149,10 +158,17 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     rc.item = i;
     std::vector<uint32_t> md, mp;
     split_pattern(pres, g.k, n, rc.surv, md, mp);
+    const size_t rebuilt = md.size() + (it.op == RS_BATCH_RECONSTRUCT ? mp.size() : 0);
+    if (rebuilt == 0) continue;
+    b->bytes += (g.k + rebuilt) * it.row_len;
+    // Missing parity of a shape with a compiled encode kernel is regenerated by that
+    // kernel after the data rows are whole, storing only the missing rows.
+    const bool regen = it.op == RS_BATCH_RECONSTRUCT && !mp.empty() && !(flags & RS_BATCH_MATRIX_ONLY) &&
+                       use_fft8(it.codec, it.row_len);
     rc.targets = md;
-    if (it.op == RS_BATCH_RECONSTRUCT) rc.targets.insert(rc.targets.end(), mp.begin(), mp.end());
+    if (it.op == RS_BATCH_RECONSTRUCT && !regen) rc.targets.insert(rc.targets.end(), mp.begin(), mp.end());
+    if (regen) regen_groups[g.fft].push_back({i, mp, md.empty()});
     if (rc.targets.empty()) continue;
-    b->bytes += (g.k + rc.targets.size()) * it.row_len;
     recon[&g].push_back(std::move(rc));
   }
   if (statuses)
@@ -265,6 +281,33 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     b->fft_items += v.size();
     fft_host.push_back(std::move(v));
   }
+  struct RegenOff {
+    const FftShape *shape;
+    size_t off, mask_off, n;
+    uint64_t groups;
+  };
+  std::vector<RegenOff> rgo;
+  for (auto &kv : regen_groups) {
+    std::vector<FftItem> v;
+    std::vector<uint32_t> masks(4 * kv.second.size(), 0u);
+    uint64_t g0 = 0;
+    for (size_t p = 0; p < kv.second.size(); p++) {
+      const Regen &rg = kv.second[p];
+      const rs_batch_item &it = items[rg.item];
+      FftItem f{};
+      f.in_base = it.d_rows;
+      f.out_base = it.d_rows + (size_t)kv.first->k * it.row_stride;
+      f.row_stride = it.row_stride;
+      f.len = it.row_len;
+      f.group_begin = g0;
+      g0 += (it.row_len + 31) / 32;
+      v.push_back(f);
+      for (uint32_t x : rg.parity) masks[4 * p + (x - kv.first->k) / 32] |= 1u << ((x - kv.first->k) % 32);
+      if (rg.only) b->fft_items++;
+    }
+    size_t off = ar.put(v.data(), v.size() * sizeof(FftItem));
+    rgo.push_back({kv.first, off, ar.put(masks.data(), masks.size() * sizeof(uint32_t)), v.size(), g0});
+  }
 
   // ---- allocate, patch device pointers, upload ----
   RSB_TRY(b->mem.ensure(std::max<size_t>(ar.host.size(), 256)));
@@ -311,7 +354,10 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
 
   for (auto &f : fgo)
     b->ffts.push_back({f.shape, reinterpret_cast<const FftItem *>(base + f.off), (uint32_t)f.n,
-                       f.groups});
+                       f.groups, nullptr});
+  for (auto &f : rgo)
+    b->regens.push_back({f.shape, reinterpret_cast<const FftItem *>(base + f.off), (uint32_t)f.n, f.groups,
+                         reinterpret_cast<const uint32_t *>(base + f.mask_off)});
   b->ragged = reinterpret_cast<const RaggedItem *>(base + ragged_off);
   b->n_ragged = (uint32_t)ragged.size();
   b->ragged_blocks = blocks;
@@ -319,7 +365,7 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
   if (b->ragged_smem > 48 * 1024)
     RSB_CU(cudaFuncSetAttribute(gf8_ragged_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)b->ragged_smem));
-  b->launches = b->ffts.size() + (b->n_ragged ? 1 : 0);
+  b->launches = b->ffts.size() + b->regens.size() + (b->n_ragged ? 1 : 0);
 
   if (!(flags & RS_BATCH_NO_GRAPH) && b->launches) {
     uint64_t before = g_launches.load();

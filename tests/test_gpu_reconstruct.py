@@ -214,7 +214,9 @@ def test_reconstruct_dev_pointers(gpu, O):
     assert np.array_equal(got, full)
 
 
-@pytest.mark.parametrize("k,m,row_len,stripes", [(32, 32, 4096, 40), (16, 16, 333, 17), (10, 10, 64, 50)])
+@pytest.mark.parametrize("k,m,row_len,stripes", [(32, 32, 4096, 40), (16, 16, 333, 17), (10, 10, 64, 50),
+                                                 (64, 64, 2048, 12), (20, 12, 1000, 20), (128, 128, 512, 6),
+                                                 (20, 10, 777, 9)])
 def test_reconstruct_batch_device(gpu, O, k, m, row_len, stripes):
     """Many stripes, each with its own pattern of 1..m erasures, in one launch."""
     import torch
@@ -228,11 +230,14 @@ def test_reconstruct_batch_device(gpu, O, k, m, row_len, stripes):
     present[0, :] = 1  # one untouched stripe
     work = full.copy()
     work[present == 0] = 0
-    d = torch.from_numpy(work).cuda()
-    st = rs_batch = gpu.ReedSolomon(k, m).reconstruct_batch_dev(d, stripes, row_len, present)
-    torch.cuda.synchronize()
-    assert st == [0] * stripes, rs_batch
-    assert np.array_equal(d.cpu().numpy(), full)
+    for route in ("auto", "fft", "matrix"):  # "fft": missing parity on the compiled kernel
+        rs = gpu.ReedSolomon(k, m)
+        rs.set_route(route)
+        d = torch.from_numpy(work).cuda()
+        st = rs.reconstruct_batch_dev(d, stripes, row_len, present)
+        torch.cuda.synchronize()
+        assert st == [0] * stripes, (route, st)
+        assert np.array_equal(d.cpu().numpy(), full), route
     # data-only: missing parity rows stay as they were (zero).
     d = torch.from_numpy(work).cuda()
     gpu.ReedSolomon(k, m).reconstruct_batch_dev(d, stripes, row_len, present, data_only=True)
@@ -240,3 +245,33 @@ def test_reconstruct_batch_device(gpu, O, k, m, row_len, stripes):
     got = d.cpu().numpy()
     assert np.array_equal(got[:, :k], full[:, :k])
     assert not got[:, k:][present[:, k:] == 0].any()
+
+
+@pytest.mark.parametrize("k,m", [(32, 32), (10, 10), (128, 128)])
+def test_reconstruct_batch_device_stores_only_missing_parity(gpu, O, k, m):
+    """Shapes with a compiled encode kernel regenerate missing parity with it, storing
+    only the missing rows: present parity rows, here deliberately inconsistent with the
+    data, are left exactly as they were, on every route."""
+    import torch
+
+    rng = np.random.default_rng(k + 7)
+    stripes, row_len = 6, 1000
+    full = np.stack([encoded(O, k, m, row_len, int(rng.integers(1 << 30))) for _ in range(stripes)])
+    present = np.ones((stripes, k + m), np.uint8)
+    work = full.copy()
+    for s in range(stripes):
+        lost = rng.choice(m, size=int(rng.integers(1, m + 1)), replace=False) + k
+        present[s, lost] = 0
+        work[s, lost] = 0
+        kept = [i for i in range(k, k + m) if present[s, i]]
+        work[s, kept] ^= 0x5A
+    want = work.copy()
+    want[present == 0] = full[present == 0]
+    for route in ("fft", "auto", "matrix"):
+        rs = gpu.ReedSolomon(k, m)
+        rs.set_route(route)
+        d = torch.from_numpy(work).cuda()
+        st = rs.reconstruct_batch_dev(d, stripes, row_len, present)
+        torch.cuda.synchronize()
+        assert st == [0] * stripes
+        assert np.array_equal(d.cpu().numpy(), want), route
