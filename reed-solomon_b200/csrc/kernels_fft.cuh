@@ -4,20 +4,23 @@
 // For a (K, K) shape with K a power of two the reference's encode program is an
 // inverse transform of the K data rows on the coset {0..K-1} (interpolation,
 // src/fft.rs:198-203) followed by a forward transform on the coset {K..2K-1}
-// (src/fft.rs:330-343); its outputs are the K parity rows in order.
+// (src/fft.rs:330-343); its outputs are the K parity rows in order. The kernels run the
+// same transform pair over a searched basis of {0..K-1} (fftc::fft_basis below), which
+// yields the same parity bytes in another register order with cheaper constants.
 //
 // Bitslicing. A thread's 32 byte columns of one shard (8 words) are transposed into
 // 8 bit planes (32 bits each); the transpose is its own inverse, so the same network
 // turns parity planes back into bytes. Multiplying a register by a constant c is then
 // the GF(2) matrix of c applied to the planes: plane b of c*x is the XOR of planes b'
 // of x for which bit b of c*2^b' is set. With c known at compile time that is a short
-// fixed XOR network (about 18 three-input LOP3 operations per multiply-accumulate on
-// 32 columns), instead of a table lookup per byte.
+// fixed XOR network (about 12 three-input LOP3 operations per multiply-accumulate on
+// 32 columns, on average over the RS(32,32) transform's constants), instead of a table
+// lookup per byte.
 //
 // Lane pairs. K registers x 8 planes do not fit one thread for K = 32, so a lane pair
 // shares each 32-column group: lane h holds program registers 2j + h. At level l >= 1 a
 // butterfly pairs registers i and i + 2^l (same lane) and its constant
-// WHAT[l][beta ^ base] depends only on register bits above l, never on bit 0, so both
+// WHAT_l(beta ^ P(base)) depends only on register bits above l, never on bit 0, so both
 // lanes run the same straight-line code with the same constants. Level 0 pairs 2j with
 // 2j + 1: the lanes swap the register with one shuffle per plane and each keeps its
 // own half of the butterfly.
