@@ -130,8 +130,9 @@ int rs8_dec_clone(const rs8_dec_t *dec, rs8_dec_t **out);
 void rs8_dec_free(rs8_dec_t *dec);
 /* ReedSolomon::encode_route, src/reedsolomon.rs:239-253 (bench/test introspection):
  * "fft-bitsliced" ((K,K), K a power of two), "generator-bitsliced" ((7,13), (10,10),
- * (14,14), (18,6), (20,12): the reference's other generated shapes, with the generator
- * compiled in) or "matrix" for this shard length. Never NULL. */
+ * (14,14), (18,6): the reference's other generated shapes; (20,12); the storage codes
+ * (4,2), (6,3), (8,4), (10,4), (12,4), (16,4), (17,3): the generator compiled in) or
+ * "matrix" for this shard length. Never NULL. */
 const char *rs8_encode_route(const rs8_t *codec, size_t len);
 /* Test/bench hook like the reference's encode_scalar/encode_forced
  * (src/reedsolomon.rs:365-424): route 0 = automatic, 1 = matrix, 2 = the shape's

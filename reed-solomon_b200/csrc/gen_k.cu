@@ -1,5 +1,5 @@
-// Instantiates the compile-time generator kernels (kernels_gen.cuh) for the shapes
-// find_fft_shape marks as generator shapes.
+// Instantiates the compile-time generator kernels (kernels_gen.cuh) for the reference's
+// other generated shapes and (20,12); the storage-code shapes are in gen_k_more.cu.
 #include "kernels_gen.cuh"
 
 namespace rsb {
@@ -15,7 +15,7 @@ cudaError_t gen8_launch(int k, int m, const FftArgs &a, const PtrTableT<PTRS> &p
   if (k == 14 && m == 14) return launch_gen8_shape<14, 14, PTRS, 256, 1>(a, pt, st);
   if (k == 18 && m == 6) return launch_gen8_shape<18, 6, PTRS, 256, 1>(a, pt, st);
   if (k == 20 && m == 12) return launch_gen8_shape<20, 12, PTRS, 256, 1>(a, pt, st);
-  return cudaErrorInvalidValue;
+  return gen8_launch_more<PTRS>(k, m, a, pt, st);
 }
 
 template cudaError_t gen8_launch<false>(int, int, const FftArgs &, const PtrTableT<false> &, cudaStream_t);

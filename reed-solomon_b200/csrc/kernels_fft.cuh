@@ -703,7 +703,7 @@ inline int sm_count() {
 
 // Shapes with a compiled bitsliced encode kernel: the FFT kernel for (K, K) with K a
 // power of two, the compile-time generator kernel (kernels_gen.cuh) for the reference's
-// other generated shapes and (20,12).
+// other generated shapes, (20,12) and common storage codes.
 struct FftShape {
   int k, m;
   bool gen;  // generator kernel (no lane-group width or launch-shape choices)
@@ -713,7 +713,8 @@ inline const FftShape *find_fft_shape(size_t k, size_t m) {
   static const FftShape shapes[] = {{2, 2, false},   {4, 4, false},   {8, 8, false},  {16, 16, false},
                                     {32, 32, false}, {64, 64, false}, {128, 128, false},
                                     {7, 13, true},   {10, 10, true},  {14, 14, true}, {18, 6, true},
-                                    {20, 12, true}};
+                                    {20, 12, true},  {4, 2, true},    {6, 3, true},   {8, 4, true},
+                                    {10, 4, true},   {12, 4, true},   {16, 4, true},  {17, 3, true}};
   for (const FftShape &s : shapes)
     if ((size_t)s.k == k && (size_t)s.m == m) return &s;
   return nullptr;

@@ -1,6 +1,7 @@
 // Compile-time generator route: GF(2^8) encode for the reference's other generated
-// shapes ((7,13), (10,10), (14,14), (18,6), src/fft_programs.rs:10-17) and (20,12),
-// bitsliced like the FFT kernels of kernels_fft.cuh.
+// shapes ((7,13), (10,10), (14,14), (18,6), src/fft_programs.rs:10-17), (20,12) and
+// common storage codes ((4,2), (6,3), (8,4), (10,4), (12,4), (16,4), (17,3)), bitsliced
+// like the FFT kernels of kernels_fft.cuh.
 //
 // The reference encodes these shapes with straight-line programs that its FFT builder
 // generated (src/fft.rs:156-592). Their outputs are the systematic generator's parity
@@ -160,6 +161,9 @@ __global__ void __launch_bounds__(THREADS, CTAS)
     });
   }
 }
+
+template <bool PTRS>
+cudaError_t gen8_launch_more(int k, int m, const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st);
 
 template <int KD, int MP, bool PTRS, int THREADS, int CTAS>
 inline cudaError_t launch_gen8_shape(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {

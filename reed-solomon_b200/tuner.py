@@ -11,7 +11,7 @@ Candidates (GF(2^8)):
   FFT route ((K,K) shapes), lane-group width narrow/wide x launch shape (threads x CTAs
   per SM) 128x3 / 128x4 / 128x2 / 256x1
   generator route (the compiled generator kernel of (7,13), (10,10), (14,14), (18,6),
-  (20,12))
+  (20,12) and the storage codes (4,2), (6,3), (8,4), (10,4), (12,4), (16,4), (17,3))
 """
 import ctypes
 import math
@@ -26,7 +26,8 @@ CONFIGS = [("matrix", 0), ("matrix", 1), ("matrix", 2), ("matrix", 3),
            ("fft", (0, 2)), ("fft", (1, 2)), ("fft", (0, 3)), ("fft", (1, 3)), ("gen", 0)]
 N_FEATURES = 5
 FFT_K = (2, 4, 8, 16, 32, 64, 128)
-GEN_SHAPES = ((7, 13), (10, 10), (14, 14), (18, 6), (20, 12))
+GEN_SHAPES = ((7, 13), (10, 10), (14, 14), (18, 6), (20, 12), (4, 2), (6, 3), (8, 4), (10, 4), (12, 4),
+              (16, 4), (17, 3))
 
 
 class Workload:

@@ -7,7 +7,8 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(7, 13), (10, 10), (14, 14), (16, 16), (18, 6), (32, 32), (20, 12), (64, 64), (128, 128)]
+SHAPES = [(7, 13), (10, 10), (14, 14), (16, 16), (18, 6), (32, 32), (20, 12), (64, 64), (128, 128), (10, 4),
+          (17, 3)]
 
 
 def make_batch(gpu, O, n_stripes, seed, max_len=8192):

@@ -34,7 +34,8 @@ def encode_gpu(rs, data, m):
 
 
 SHAPES = [(7, 13), (10, 10), (20, 10), (4, 2), (6, 4), (17, 17), (32, 32), (16, 16), (14, 14),
-          (18, 6), (20, 12), (1, 1), (2, 2), (8, 8), (64, 64), (128, 128), (255, 1), (1, 255)]
+          (18, 6), (20, 12), (1, 1), (2, 2), (8, 8), (64, 64), (128, 128), (255, 1), (1, 255),
+          (6, 3), (8, 4), (10, 4), (12, 4), (16, 4), (17, 3)]
 LENGTHS = [1, 15, 16, 17, 31, 32, 33, 63, 64, 65, 100, 987, 1024, 4103, 65536]
 
 
@@ -169,6 +170,8 @@ def test_encode_route_introspection(gpu):
     assert gpu.ReedSolomon(10, 10).encode_route(1 << 16) == "generator-bitsliced"
     assert gpu.ReedSolomon(10, 10).encode_route(32) == "matrix"  # under two column groups
     assert gpu.ReedSolomon(20, 10).encode_route(1 << 20) == "matrix"
+    for k, m in [(4, 2), (6, 3), (8, 4), (10, 4), (12, 4), (16, 4), (17, 3)]:
+        assert gpu.ReedSolomon(k, m).encode_route(4096) == "generator-bitsliced", (k, m)
 
 
 def test_clone_and_eq(gpu):
