@@ -45,6 +45,9 @@ struct rs8_decoder {
 namespace rsb {
 
 bool use_fft8(const rs8_codec *c, size_t len);
+// Whether regenerating `missing_parity` parity rows with the shape's compiled kernel
+// beats applying them on the matrix route (route 2 forces it).
+bool regen_parity_pays(const Gen8 &g, size_t missing_parity, int route);
 int encode8_strided(rs8_codec *c, const uint8_t *in_base, uint64_t in_row, uint64_t in_stripe, uint8_t *out_base,
                     uint64_t out_row, uint64_t out_stripe, size_t n_stripes, size_t len, cudaStream_t st);
 int launch_gf8(const ApplyArgs &a, const PtrTable *pt, bool verify, cudaStream_t st);

@@ -437,10 +437,15 @@ struct FftArgs {
   // Parity rows to store, 4 words (rows 0..127) per stripe, or per item in the ragged
   // form; null stores every row. Reconstruct uses it to rebuild only the missing parity.
   const uint32_t *store_mask;
+  // The same for a single stripe, passed by value (use_store_bits != 0).
+  uint32_t store_bits[4];
+  int use_store_bits;
 };
 
 __device__ __forceinline__ bool fft_store_row(const FftArgs &a, uint32_t unit, uint32_t row) {
-  return !a.store_mask || ((a.store_mask[4 * (uint64_t)unit + (row >> 5)] >> (row & 31)) & 1u);
+  if (a.store_mask) return (a.store_mask[4 * (uint64_t)unit + (row >> 5)] >> (row & 31)) & 1u;
+  if (a.use_store_bits) return (a.store_bits[row >> 5] >> (row & 31)) & 1u;
+  return true;
 }
 
 // Where one lane pair's 32-column group lives.
@@ -875,8 +880,14 @@ inline int launch_fft8_items(const FftShape &sh, const FftItem *d_items, uint32_
   return launch_fft_any<false>(sh, a, pt, st);
 }
 
-inline int launch_fft8_ptrs(const FftShape &sh, uint8_t *const *shards, uint64_t len, cudaStream_t st) {
+// store_bits (4 words, parity rows 0..127): store only those parity rows; null: all.
+inline int launch_fft8_ptrs(const FftShape &sh, uint8_t *const *shards, uint64_t len, cudaStream_t st,
+                            const uint32_t *store_bits = nullptr) {
   FftArgs a{};
+  if (store_bits) {
+    a.use_store_bits = 1;
+    for (int w = 0; w < 4; w++) a.store_bits[w] = store_bits[w];
+  }
   a.len = len;
   a.n_stripes = 1;
   a.groups_per_stripe = (uint32_t)((len + 31) / 32);

@@ -151,6 +151,19 @@ bool use_fft8(const rs8_codec *c, size_t len) {
   return len >= 64;
 }
 
+// The compiled kernel rereads all k data rows and does an encode's work, about (k+m)
+// bytes per column at its rate (~3.5 TB/s; ~2.1 at K = 64, ~1.4 at K = 128), to save
+// missing_parity * k matrix coefficients per column (2 LOP3 per byte each, ~11 Tops/s):
+// it pays from missing_parity * k ~ 1.6 (k+m) at 3.5 TB/s. Measured on B200: RS(32,32)
+// with 8 missing parity rows +17% at 1 MiB shards, (64,64) with 16 +51%, (10,4) with 1
+// -15%. The factors below keep a margin.
+bool regen_parity_pays(const Gen8 &g, size_t missing_parity, int route) {
+  if (!g.fft || missing_parity == 0 || route == 1) return false;
+  if (route == 2) return true;
+  const size_t factor = g.k >= 128 ? 4 : g.k >= 64 ? 3 : 2;
+  return missing_parity * g.k >= factor * (g.k + g.m);
+}
+
 int encode8_strided(rs8_codec *c, const uint8_t *in_base, uint64_t in_row, uint64_t in_stripe,
                            uint8_t *out_base, uint64_t out_row, uint64_t out_stripe, size_t n_stripes,
                            size_t len, cudaStream_t st) {
@@ -226,10 +239,11 @@ static int plan8_for(const Gen8 &g, PlanCache &cache, Exec &ex, const Presence &
 }
 
 // Shared body of every GF(2^8) reconstruct (src/reedsolomon.rs:615-641, :829-891).
-// With `dev` the shard pointers are device pointers and work is enqueued on `st`.
+// With `dev` the shard pointers are device pointers and work is enqueued on `st`;
+// `route` is the codec's (0 automatic, 1 matrix, 2 compiled kernel).
 static int reconstruct8(const Gen8 &g, PlanCache *cache, const Plan *fixed, Exec &ex,
                         uint8_t *const *shards, const size_t *lens, const uint8_t *present,
-                        size_t n_shards, bool data_only, bool dev, cudaStream_t st) {
+                        size_t n_shards, bool data_only, bool dev, cudaStream_t st, int route = 0) {
   size_t n = g.k + g.m;
   if (!shards || !lens || !present) return RS_ERR_INVALID_ARGUMENT;
   if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
@@ -260,9 +274,23 @@ static int reconstruct8(const Gen8 &g, PlanCache *cache, const Plan *fixed, Exec
   a.n_stripes = 1;
   if (dev) {
     RSB_CU(cudaSetDevice(g.device));
-    for (size_t t = 0; t < g.k; t++) pt.in[t] = shards[plan->survivors[t]];
-    for (size_t j = 0; j < rows; j++) pt.out[j] = shards[outs[j]];
-    return launch_gf8(a, &pt, false, st);
+    // Shards of at least 64 KiB on a shape with a compiled kernel: the matrix route
+    // rebuilds the missing data rows (its plan's leading rows), then the compiled
+    // kernel regenerates the missing parity from the whole data rows, storing only
+    // those rows. Smaller calls are latency-bound and keep the single launch.
+    const bool split = !data_only && len >= 64 && (route == 2 || len >= ((size_t)64 << 10)) &&
+                       regen_parity_pays(g, plan->missing_parity.size(), route);
+    const size_t mrows = split ? plan->missing_data.size() : rows;
+    if (mrows) {
+      a.rows = (uint32_t)mrows;
+      for (size_t t = 0; t < g.k; t++) pt.in[t] = shards[plan->survivors[t]];
+      for (size_t j = 0; j < mrows; j++) pt.out[j] = shards[outs[j]];
+      RSB_TRY(launch_gf8(a, &pt, false, st));
+    }
+    if (!split) return RS_OK;
+    uint32_t bits[4] = {0, 0, 0, 0};
+    for (uint32_t x : plan->missing_parity) bits[(x - g.k) / 32] |= 1u << ((x - g.k) % 32);
+    return launch_fft8_ptrs(*g.fft, shards, len, st, bits);
   }
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
@@ -787,7 +815,7 @@ int rs8_reconstruct_dev(rs8_t *c, uint8_t *const *d_shards, const size_t *lens, 
                         size_t n_shards, int data_only, void *stream) {
   if (!c) return RS_ERR_INVALID_ARGUMENT;
   return reconstruct8(*c->gen, c->plans.get(), nullptr, *c->exec, d_shards, lens, present, n_shards,
-                      data_only != 0, true, (cudaStream_t)stream);
+                      data_only != 0, true, (cudaStream_t)stream, c->route.load());
 }
 
 int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, size_t n_stripes,
@@ -803,9 +831,9 @@ int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, s
   // Where the shape has a compiled encode kernel, missing parity is regenerated by it
   // from the data rows once they are whole, storing only the missing rows: the matrix
   // route then applies (missing data) x k decode coefficients per column instead of
-  // (missing data + missing parity) x k. Measured on B200 (RS(32,32), 1..m erasures per
-  // stripe, both forms timed in one process): +10% at 4 KiB shards, +21% at 16 KiB,
-  // +28% at 64 KiB.
+  // (missing data + missing parity) x k, where that pays (regen_parity_pays). Measured
+  // on B200 (RS(32,32), 1..m erasures per stripe, both forms timed in one process):
+  // +10% at 4 KiB shards, +21% at 16 KiB, +28% at 64 KiB.
   const bool split = !data_only && use_fft8(c, row_len);
   // Host side: per-stripe survivors and targets.
   std::vector<uint16_t> surv(n_stripes * k), targ(n_stripes * g.m), ntarg(n_stripes);
@@ -834,7 +862,7 @@ int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, s
     for (size_t t = 0; t < k; t++) surv[s * k + t] = (uint16_t)s_surv[t];
     size_t r = 0;
     for (uint32_t x : s_md) targ[s * g.m + r++] = (uint16_t)x;
-    if (split && !s_mp.empty()) {
+    if (split && regen_parity_pays(g, s_mp.size(), c->route.load())) {
       FftItem f{};
       f.in_base = d_rows + s * stripe_stride;
       f.out_base = d_rows + s * stripe_stride + k * row_len;

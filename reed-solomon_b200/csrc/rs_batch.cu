@@ -162,9 +162,10 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     if (rebuilt == 0) continue;
     b->bytes += (g.k + rebuilt) * it.row_len;
     // Missing parity of a shape with a compiled encode kernel is regenerated by that
-    // kernel after the data rows are whole, storing only the missing rows.
-    const bool regen = it.op == RS_BATCH_RECONSTRUCT && !mp.empty() && !(flags & RS_BATCH_MATRIX_ONLY) &&
-                       use_fft8(it.codec, it.row_len);
+    // kernel after the data rows are whole, storing only the missing rows, where that
+    // beats the matrix route (regen_parity_pays).
+    const bool regen = it.op == RS_BATCH_RECONSTRUCT && !(flags & RS_BATCH_MATRIX_ONLY) &&
+                       use_fft8(it.codec, it.row_len) && regen_parity_pays(g, mp.size(), it.codec->route.load());
     rc.targets = md;
     if (it.op == RS_BATCH_RECONSTRUCT && !regen) rc.targets.insert(rc.targets.end(), mp.begin(), mp.end());
     if (regen) regen_groups[g.fft].push_back({i, mp, md.empty()});

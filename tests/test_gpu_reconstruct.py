@@ -275,3 +275,33 @@ def test_reconstruct_batch_device_stores_only_missing_parity(gpu, O, k, m):
         torch.cuda.synchronize()
         assert st == [0] * stripes
         assert np.array_equal(d.cpu().numpy(), want), route
+
+
+@pytest.mark.parametrize("k,m,length", [(32, 32, 70000), (10, 4, 5000), (16, 16, 65536)])
+def test_reconstruct_dev_stores_only_missing_parity(gpu, O, k, m, length):
+    """Single-stripe device reconstruct on a shape with a compiled encode kernel: large
+    shards (and the forced compiled route) rebuild missing data on the matrix route and
+    regenerate missing parity with the compiled kernel, which leaves present parity rows
+    untouched (the ones the decoder does not read are made inconsistent here, so a stray
+    write would show); every route gives the same bytes."""
+    import torch
+
+    rng = np.random.default_rng(k * 3 + length)
+    full = encoded(O, k, m, length, 99)
+    n = k + m
+    lost = sorted(rng.choice(n, size=m, replace=False).tolist())
+    work = full.copy()
+    work[lost] = 0
+    survivors = [i for i in range(n) if i not in lost][:k]  # the first k present are read
+    unread = [i for i in range(k, n) if i not in lost and i not in survivors]
+    work[unread] ^= 0x3C
+    want = work.copy()
+    want[lost] = full[lost]
+    for route in ("auto", "fft", "matrix"):
+        rs = gpu.ReedSolomon(k, m)
+        rs.set_route(route)
+        bufs = [torch.from_numpy(work[i].copy()).cuda() for i in range(n)]
+        rs.reconstruct_dev(bufs, [i not in lost for i in range(n)], length)
+        torch.cuda.synchronize()
+        got = np.array([b.cpu().numpy() for b in bufs])
+        assert np.array_equal(got, want), route
