@@ -132,7 +132,8 @@ void rs8_dec_free(rs8_dec_t *dec);
  * "fft-bitsliced" ((K,K), K a power of two), "generator-bitsliced" ((7,13), (10,10),
  * (14,14), (18,6): the reference's other generated shapes; (20,12); the storage codes
  * (4,2), (6,3), (8,4), (10,4), (12,4), (16,4), (17,3): the generator compiled in) or
- * "matrix" for this shard length. Never NULL. */
+ * "matrix" for this shard length, for 16-byte aligned rows (on unaligned rows the
+ * generator shapes take the matrix kernel). Never NULL. */
 const char *rs8_encode_route(const rs8_t *codec, size_t len);
 /* Test/bench hook like the reference's encode_scalar/encode_forced
  * (src/reedsolomon.rs:365-424): route 0 = automatic, 1 = matrix, 2 = the shape's
@@ -393,13 +394,15 @@ int rs_decode_rows(int field, size_t k, size_t m, const uint8_t *present, uint16
 /* Number of this library's kernel launches so far in this process. */
 uint64_t rs_kernel_launch_count(void);
 /* Tuning hook (autotuner): launch shape of the (k,k) bitsliced FFT kernel for batched
- * calls, 0..rs_fft_variant_count()-1 (CTAs per SM). Returns the previous value, or -1
- * when out of range or (k,k) has no FFT kernel. */
+ * calls, 0..rs_fft_variant_count()-1 (CTAs per SM), or -1 for the automatic choice (the
+ * default: this shape's tuned value on 16-byte aligned rows, a wide-lane shape on
+ * unaligned ones). Setting a value fixes the shape for every call. Returns the previous
+ * value, or -1 when out of range or (k,k) has no FFT kernel. */
 int rs_set_fft_variant(size_t k, int variant);
 int rs_fft_variant_count(void);
 /* Tuning hook: lane-group width of the (k,k) FFT kernel, 0 = narrow, 1 = wide (more
- * lanes per 32-column group, fewer registers per lane). Returns the previous value,
- * or -1 when (k,k) has no FFT kernel. */
+ * lanes per 32-column group, fewer registers per lane), -1 = automatic (as above).
+ * Returns the previous value, or -1 when (k,k) has no FFT kernel. */
 int rs_set_fft_lanes(size_t k, int wide);
 /* Tuning hook: tile shape of the matrix kernel for batched and single calls
  * (parity rows per thread x output rows per CTA), 0..rs_matrix_variant_count()-1. */

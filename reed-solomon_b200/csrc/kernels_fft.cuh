@@ -689,12 +689,27 @@ __global__ void __launch_bounds__(THREADS, CTAS)
 // 1 MiB shards per launch): K = 4, 8 and 16 prefer four 128-thread CTAs per SM; K = 32, 64
 // and 128, whose slots need 255 registers, one 256-thread CTA per SM (10-12% above two
 // 128-thread CTAs with the same registers and staging).
+constexpr int kFftVariantDefault[8] = {0, 0, 1, 1, 1, 3, 3, 3};
 inline int &fft_variant_for(int K) {
   static int v[8] = {0, 0, 1, 1, 1, 3, 3, 3};
   int l = 0;
   while ((1 << l) < K) l++;
   return v[l & 7];
 }
+
+// Automatic launch shape (the default; cleared by an explicit rs_set_fft_variant or
+// rs_set_fft_lanes, restored by passing -1): on strided rows that are not 16-byte
+// aligned, every 32-byte group takes the per-byte staging path and more threads per
+// group win. Measured on B200 (rows of 65537 bytes, 2^12..2^16 groups): wide lane
+// groups with four 128-thread CTAs per SM at K = 64 and 128, with two at K = 16 and
+// 32, came within 0-22% of the best shape where the aligned defaults lost 3-146%.
+inline bool &fft_shape_auto(int K) {
+  static bool a[8] = {true, true, true, true, true, true, true, true};
+  int l = 0;
+  while ((1 << l) < K) l++;
+  return a[l & 7];
+}
+constexpr int fft_unaligned_variant(int K) { return K >= 64 ? 1 : 2; }
 
 inline int sm_count() {
   static int n = 0;
@@ -730,6 +745,7 @@ constexpr int fft_w_lo(int K) { return K <= 8 ? 1 : K <= 32 ? 1 : K == 64 ? 2 : 
 constexpr int fft_w_hi(int K) { return K <= 8 ? 1 : K <= 32 ? 2 : K == 64 ? 3 : 4; }
 
 // Selected lane-group width per K: 0 = fft_w_lo, 1 = fft_w_hi (rs_set_fft_lanes).
+constexpr int kFftLanesDefault[8] = {0, 0, 0, 0, 0, 0, 0, 1};
 inline int &fft_lanes_choice(int K) {
   static int c[8] = {0, 0, 0, 0, 0, 0, 0, 1};  // narrow groups measured fastest but for K = 128
   int l = 0;
@@ -754,24 +770,35 @@ inline cudaError_t launch_fft_kwv(const FftArgs &a, const PtrTableT<PTRS> &pt, c
 }
 
 template <int K, int W, bool PTRS>
-inline cudaError_t launch_fft_kw(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
+inline cudaError_t launch_fft_kw(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st, int variant) {
   if constexpr (PTRS) {
     return launch_fft_kwv<K, W, PTRS, 0>(a, pt, st);  // single-stripe calls
   } else {
-    if (fft_variant_for(K) == 1) return launch_fft_kwv<K, W, PTRS, 1>(a, pt, st);
-    if (fft_variant_for(K) == 2) return launch_fft_kwv<K, W, PTRS, 2>(a, pt, st);
-    if (fft_variant_for(K) == 3) return launch_fft_kwv<K, W, PTRS, 3>(a, pt, st);
+    if (variant == 1) return launch_fft_kwv<K, W, PTRS, 1>(a, pt, st);
+    if (variant == 2) return launch_fft_kwv<K, W, PTRS, 2>(a, pt, st);
+    if (variant == 3) return launch_fft_kwv<K, W, PTRS, 3>(a, pt, st);
     return launch_fft_kwv<K, W, PTRS, 0>(a, pt, st);
   }
 }
 
 template <int K, bool PTRS>
 inline cudaError_t launch_fft_k(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
+  int wide = fft_lanes_choice(K), variant = fft_variant_for(K);
+  if constexpr (!PTRS) {
+    const bool unaligned =
+        !a.items && ((reinterpret_cast<uintptr_t>(a.in_base) | reinterpret_cast<uintptr_t>(a.out_base) |
+                      a.in_row_stride | a.in_stripe_stride | a.out_row_stride | a.out_stripe_stride) &
+                     15u);
+    if (K >= 16 && unaligned && fft_shape_auto(K)) {
+      wide = 1;
+      variant = fft_unaligned_variant(K);
+    }
+  }
   if constexpr (fft_w_lo(K) == fft_w_hi(K)) {
-    return launch_fft_kw<K, fft_w_lo(K), PTRS>(a, pt, st);
+    return launch_fft_kw<K, fft_w_lo(K), PTRS>(a, pt, st, variant);
   } else {
-    if (fft_lanes_choice(K)) return launch_fft_kw<K, fft_w_hi(K), PTRS>(a, pt, st);
-    return launch_fft_kw<K, fft_w_lo(K), PTRS>(a, pt, st);
+    if (wide) return launch_fft_kw<K, fft_w_hi(K), PTRS>(a, pt, st, variant);
+    return launch_fft_kw<K, fft_w_lo(K), PTRS>(a, pt, st, variant);
   }
 }
 

@@ -132,7 +132,8 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     const size_t n = g.k + g.m;
     if (it.op == RS_BATCH_ENCODE) {
       b->bytes += n * it.row_len;
-      if (!(flags & RS_BATCH_MATRIX_ONLY) && use_fft8(it.codec, it.row_len))
+      if (!(flags & RS_BATCH_MATRIX_ONLY) &&
+          use_fft8(it.codec, it.row_len, reinterpret_cast<uintptr_t>(it.d_rows) | it.row_stride))
         fft_groups[g.fft].push_back(i);
       else
         matrix_encodes.push_back(i);
@@ -165,7 +166,8 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     // kernel after the data rows are whole, storing only the missing rows, where that
     // beats the matrix route (regen_parity_pays).
     const bool regen = it.op == RS_BATCH_RECONSTRUCT && !(flags & RS_BATCH_MATRIX_ONLY) &&
-                       use_fft8(it.codec, it.row_len) && regen_parity_pays(g, mp.size(), it.codec->route.load());
+                       use_fft8(it.codec, it.row_len, reinterpret_cast<uintptr_t>(it.d_rows) | it.row_stride) &&
+                       regen_parity_pays(g, mp.size(), it.codec->route.load());
     rc.targets = md;
     if (it.op == RS_BATCH_RECONSTRUCT && !regen) rc.targets.insert(rc.targets.end(), mp.begin(), mp.end());
     if (regen) regen_groups[g.fft].push_back({i, mp, md.empty()});

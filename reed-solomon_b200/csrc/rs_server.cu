@@ -729,7 +729,10 @@ static void launch_group(rs_server *s, Group *g) {
 static bool route_fft(const rs_server *s, const rs_request &r) {
   const FftShape *sh = find_fft_shape(r.data_shards, r.parity_shards);
   if (!sh || r.op != RS_BATCH_ENCODE) return false;
-  if (sh->gen) return r.row_len >= 64;  // no per-size hints for generator shapes
+  // Generator shapes: no per-size hints; rows must be 16-byte aligned (host rows are
+  // staged at row_len apart in the arena).
+  if (sh->gen)
+    return r.row_len >= 64 && !((r.row_len | (r.rows_on_host ? 0 : reinterpret_cast<uintptr_t>(r.rows))) & 15);
   int kl = 0;
   while ((1 << (kl + 1)) <= sh->k) kl++;
   int bl = 0;
