@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--requests", type=int, default=400, help="requests of the serve workload")
     ap.add_argument("--rs16", default=None, help="rs16 workload: one shape K,M,STRIPES instead of both")
     ap.add_argument("--mixed-stripes", type=int, default=10000, help="stripes of the mixed workload")
+    ap.add_argument("--mixed-packed", action="store_true",
+                    help="mixed workload: rows packed back to back at their (odd) lengths")
     ap.add_argument("--stripes-shapes", default=None,
                     help="stripes workload: shapes K,M separated by '/' (default 32,32/16,16)")
     ap.add_argument("--stripes-sizes", default=None,
@@ -347,7 +349,7 @@ def run_workload(args):
             line = {"metric": "RS(k,m) encode/reconstruct GB/s, %d stripes per launch" % args.stripes_count,
                     "unit": "GB/s", "results": res}
         elif args.workload == "mixed":
-            res = workloads.mixed_batch(n=args.mixed_stripes)
+            res = workloads.mixed_batch(n=args.mixed_stripes, packed=args.mixed_packed)
             line = {"metric": "mixed-shape batch GB/s, batched+tuned vs plain", "unit": "GB/s",
                     "value": res["batched_gbs"], "results": res}
         elif args.workload == "rs16":

@@ -132,8 +132,7 @@ void rs8_dec_free(rs8_dec_t *dec);
  * "fft-bitsliced" ((K,K), K a power of two), "generator-bitsliced" ((7,13), (10,10),
  * (14,14), (18,6): the reference's other generated shapes; (20,12); the storage codes
  * (4,2), (6,3), (8,4), (10,4), (12,4), (16,4), (17,3): the generator compiled in) or
- * "matrix" for this shard length, for 16-byte aligned rows (on unaligned rows the
- * generator shapes take the matrix kernel). Never NULL. */
+ * "matrix" for this shard length. Never NULL. */
 const char *rs8_encode_route(const rs8_t *codec, size_t len);
 /* Test/bench hook like the reference's encode_scalar/encode_forced
  * (src/reedsolomon.rs:365-424): route 0 = automatic, 1 = matrix, 2 = the shape's

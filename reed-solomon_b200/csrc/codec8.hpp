@@ -44,8 +44,7 @@ struct rs8_decoder {
 
 namespace rsb {
 
-// align: the OR of the rows' base addresses and strides (0 when unknown / aligned).
-bool use_fft8(const rs8_codec *c, size_t len, uintptr_t align = 0);
+bool use_fft8(const rs8_codec *c, size_t len);
 // Whether regenerating `missing_parity` parity rows with the shape's compiled kernel
 // beats applying them on the matrix route (route 2 forces it).
 bool regen_parity_pays(const Gen8 &g, size_t missing_parity, int route);

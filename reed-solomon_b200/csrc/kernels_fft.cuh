@@ -440,6 +440,8 @@ struct FftArgs {
   // The same for a single stripe, passed by value (use_store_bits != 0).
   uint32_t store_bits[4];
   int use_store_bits;
+  // Ragged form: some item's rows are not 16-byte aligned (chooses the launch shape).
+  int items_unaligned;
 };
 
 __device__ __forceinline__ bool fft_store_row(const FftArgs &a, uint32_t unit, uint32_t row) {
@@ -522,30 +524,111 @@ __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Byte paths for the last, partial group of a shard or unaligned rows, kept out of
-// line: the unrolled per-shard code then holds a call instead of a byte loop, so these
-// rarely taken fallbacks do not fill the instruction cache.
-static __device__ __noinline__ void stage32_bytes(uint8_t *slot, int half, const uint8_t *p, uint64_t remain) {
-  uint32_t w[8];
-  load32(p, remain, w);
-  *reinterpret_cast<uint4 *>(slot) = make_uint4(w[0], w[1], w[2], w[3]);
-  *reinterpret_cast<uint4 *>(slot + half) = make_uint4(w[4], w[5], w[6], w[7]);
+// Slow paths, for the last, partial group of a shard and for unaligned rows, are kept
+// out of line: the unrolled per-shard code then holds one call instead of a byte loop,
+// so these rarely taken paths do not fill the instruction cache.
+// Unaligned rows (packed rows whose length is not a multiple of 16). A group that starts
+// at least 32 bytes into its row and has at least 48 row bytes from its start is read
+// as the three 16-byte aligned blocks around it, which then lie inside the row, and
+// shifted into place: 3 vector loads instead of 32 byte loads. o = p mod 16.
+static __device__ __forceinline__ void stage32_window(uint8_t *slot, int half, const uint8_t *p) {
+  const uint32_t o = (uint32_t)((uintptr_t)p & 15u), q = o >> 2, r = (o & 3u) * 8u;
+  const uint4 *blk = reinterpret_cast<const uint4 *>(p - o);
+  const uint4 b0 = __ldg(blk), b1 = __ldg(blk + 1), b2 = __ldg(blk + 2);
+  const uint32_t w[12] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w, b2.x, b2.y, b2.z, b2.w};
+  uint32_t v[9];  // v[i] = w[q + i], selected without indexing registers at run time
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    uint32_t x = w[i];
+    if (i + 1 < 12) x = q == 1 ? w[i + 1] : x;
+    if (i + 2 < 12) x = q == 2 ? w[i + 2] : x;
+    if (i + 3 < 12) x = q == 3 ? w[i + 3] : x;
+    v[i] = x;
+  }
+  uint32_t out[8];  // bytes o + 4i .. o + 4i + 3 of the window
+#pragma unroll
+  for (int i = 0; i < 8; i++) out[i] = __funnelshift_r(v[i], v[i + 1], r);
+  *reinterpret_cast<uint4 *>(slot) = make_uint4(out[0], out[1], out[2], out[3]);
+  *reinterpret_cast<uint4 *>(slot + half) = make_uint4(out[4], out[5], out[6], out[7]);
 }
 
-static __device__ __noinline__ void store32_bytes(uint8_t *p, uint64_t remain, uint4 lo, uint4 hi) {
-  const uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
-  store32(p, remain, w);
+// Store a whole group (32 bytes) at an unaligned p without touching bytes outside it:
+// the group's bytes are placed at offset o of the 48-byte aligned window around p; the
+// middle block is one 16-byte store, the two edge blocks go out as the naturally
+// aligned words, halfwords and bytes that lie inside the group.
+static __device__ __forceinline__ void store32_window(uint8_t *p, uint4 lo, uint4 hi) {
+  const uint32_t o = (uint32_t)((uintptr_t)p & 15u), q = o >> 2, r = (o & 3u) * 8u;
+  uint8_t *base = p - o;
+  const uint32_t in[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+  uint32_t u[12];  // u[j] = in[j - q] (0 outside 0..7)
+#pragma unroll
+  for (int j = 0; j < 12; j++) {
+    uint32_t x = j < 8 ? in[j] : 0u;
+    x = q == 1 ? (j >= 1 && j - 1 < 8 ? in[j - 1] : 0u) : x;
+    x = q == 2 ? (j >= 2 && j - 2 < 8 ? in[j - 2] : 0u) : x;
+    x = q == 3 ? (j >= 3 && j - 3 < 8 ? in[j - 3] : 0u) : x;
+    u[j] = x;
+  }
+  uint32_t W[12];  // window bytes 4i .. 4i + 3
+#pragma unroll
+  for (int i = 0; i < 12; i++) W[i] = __funnelshift_l(i ? u[i - 1] : 0u, u[i], r);
+  // Window bytes [o, o + 32) belong to the group.
+#pragma unroll
+  for (int i = 0; i < 12; i++) {
+    if (i >= 4 && i < 8) continue;  // the middle block, below
+    const uint32_t b0 = 4u * i, b1 = b0 + 4u, g0 = o, g1 = o + 32u;
+    if (b0 >= g0 && b1 <= g1) {
+      *reinterpret_cast<uint32_t *>(base + b0) = W[i];
+    } else if (b1 > g0 && b0 < g1) {  // a partial word: bytes [max(b0,g0), min(b1,g1))
+      const uint32_t s0 = b0 > g0 ? b0 : g0, s1 = b1 < g1 ? b1 : g1;
+      uint32_t x = s0;
+      if ((x & 1u) && x < s1) {
+        base[x] = (uint8_t)(W[i] >> (8u * (x - b0)));
+        x++;
+      }
+      if (x + 2 <= s1) {
+        *reinterpret_cast<uint16_t *>(base + x) = (uint16_t)(W[i] >> (8u * (x - b0)));
+        x += 2;
+      }
+      if (x < s1) base[x] = (uint8_t)(W[i] >> (8u * (x - b0)));
+    }
+  }
+  *reinterpret_cast<uint4 *>(base + 16) = make_uint4(W[4], W[5], W[6], W[7]);
 }
 
-// Stage the 32 bytes at p (remain of them valid) into this thread's slot: two async
-// 16-byte copies when aligned and whole, else the zero-filled byte path.
+// Stage the 32 bytes at p (remain of them valid, col bytes of the row before p) into
+// this thread's slot: two async 16-byte copies when aligned and whole, the aligned
+// window for interior groups of unaligned rows, else the zero-filled byte path.
+static __device__ __noinline__ void stage32_slow(uint8_t *slot, int half, const uint8_t *p, uint64_t remain,
+                                                 uint64_t col) {
+  if (col >= 32 && remain >= 48) {
+    stage32_window(slot, half, p);
+  } else {
+    uint32_t w[8];
+    load32(p, remain, w);
+    *reinterpret_cast<uint4 *>(slot) = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4 *>(slot + half) = make_uint4(w[4], w[5], w[6], w[7]);
+  }
+}
+
 template <int HALF>
-__device__ __forceinline__ void stage32(uint8_t *slot, const uint8_t *p, uint64_t remain) {
+__device__ __forceinline__ void stage32(uint8_t *slot, const uint8_t *p, uint64_t remain, uint64_t col) {
   if (remain >= 32 && (((uintptr_t)p & 15u) == 0)) {
     cp_async16(slot, p);
     cp_async16(slot + HALF, p + 16);
   } else {
-    stage32_bytes(slot, HALF, p, remain);
+    stage32_slow(slot, HALF, p, remain, col);
+  }
+}
+
+// Store the 32 bytes of a group at p (remain of them valid) on the slow paths: one
+// out-of-line call, so the unrolled store loops carry a single call per slot.
+static __device__ __noinline__ void store32_any(uint8_t *p, uint64_t remain, uint4 lo, uint4 hi) {
+  if (remain >= 32) {
+    store32_window(p, lo, hi);
+  } else {
+    const uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+    store32(p, remain, w);
   }
 }
 
@@ -620,7 +703,7 @@ __global__ void __launch_bounds__(THREADS, CTAS)
       }
     } else {
 #pragma unroll 1
-      for (int j = 0; j < S; j++) stage32<St::kHalf>(mine + j * St::kSlot, in_ptr(l, j) + l.col, l.remain);
+      for (int j = 0; j < S; j++) stage32<St::kHalf>(mine + j * St::kSlot, in_ptr(l, j) + l.col, l.remain, l.col);
     }
     cp_async_commit();
   };
@@ -677,7 +760,7 @@ __global__ void __launch_bounds__(THREADS, CTAS)
           *reinterpret_cast<uint4 *>(row + col) = lo;
           *reinterpret_cast<uint4 *>(row + col + 16) = hi;
         } else {
-          store32_bytes(row + col, remain, lo, hi);
+          store32_any(row + col, remain, lo, hi);
         }
       }
     }
@@ -699,17 +782,18 @@ inline int &fft_variant_for(int K) {
 
 // Automatic launch shape (the default; cleared by an explicit rs_set_fft_variant or
 // rs_set_fft_lanes, restored by passing -1): on strided rows that are not 16-byte
-// aligned, every 32-byte group takes the per-byte staging path and more threads per
+// aligned, every 32-byte group takes the unaligned staging paths and more threads per
 // group win. Measured on B200 (rows of 65537 bytes, 2^12..2^16 groups): wide lane
-// groups with four 128-thread CTAs per SM at K = 64 and 128, with two at K = 16 and
-// 32, came within 0-22% of the best shape where the aligned defaults lost 3-146%.
+// groups with four 128-thread CTAs per SM were the best shape from 2^14 groups at
+// every K >= 16 (up to 63% off the best at 2^12), where the aligned defaults lost
+// 16-89%.
 inline bool &fft_shape_auto(int K) {
   static bool a[8] = {true, true, true, true, true, true, true, true};
   int l = 0;
   while ((1 << l) < K) l++;
   return a[l & 7];
 }
-constexpr int fft_unaligned_variant(int K) { return K >= 64 ? 1 : 2; }
+constexpr int fft_unaligned_variant(int K) { return K >= 16 ? 1 : 0; }
 
 inline int sm_count() {
   static int n = 0;
@@ -786,9 +870,10 @@ inline cudaError_t launch_fft_k(const FftArgs &a, const PtrTableT<PTRS> &pt, cud
   int wide = fft_lanes_choice(K), variant = fft_variant_for(K);
   if constexpr (!PTRS) {
     const bool unaligned =
-        !a.items && ((reinterpret_cast<uintptr_t>(a.in_base) | reinterpret_cast<uintptr_t>(a.out_base) |
-                      a.in_row_stride | a.in_stripe_stride | a.out_row_stride | a.out_stripe_stride) &
-                     15u);
+        a.items ? a.items_unaligned != 0
+                : ((reinterpret_cast<uintptr_t>(a.in_base) | reinterpret_cast<uintptr_t>(a.out_base) |
+                    a.in_row_stride | a.in_stripe_stride | a.out_row_stride | a.out_stripe_stride) &
+                   15u) != 0;
     if (K >= 16 && unaligned && fft_shape_auto(K)) {
       wide = 1;
       variant = fft_unaligned_variant(K);
@@ -897,12 +982,14 @@ inline int launch_fft8(const FftShape &sh, const uint8_t *in_base, uint64_t in_r
 
 // Ragged batch of (K, K) stripes described by a device item array.
 inline int launch_fft8_items(const FftShape &sh, const FftItem *d_items, uint32_t n_items,
-                             uint64_t total_groups, cudaStream_t st, const uint32_t *store_mask = nullptr) {
+                             uint64_t total_groups, cudaStream_t st, const uint32_t *store_mask = nullptr,
+                             bool items_unaligned = false) {
   FftArgs a{};
   a.items = d_items;
   a.n_items = n_items;
   a.total_groups = total_groups;
   a.store_mask = store_mask;
+  a.items_unaligned = items_unaligned;
   PtrTableT<false> pt{};
   return launch_fft_any<false>(sh, a, pt, st);
 }

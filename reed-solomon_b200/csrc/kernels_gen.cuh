@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(THREADS, CTAS)
       }
     } else {
 #pragma unroll 1
-      for (int i = 0; i < KD; i++) stage32<St::kHalf>(mine + i * St::kSlot, in_ptr(l, i) + l.col, l.remain);
+      for (int i = 0; i < KD; i++) stage32<St::kHalf>(mine + i * St::kSlot, in_ptr(l, i) + l.col, l.remain, l.col);
     }
     cp_async_commit();
   };
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(THREADS, CTAS)
         *reinterpret_cast<uint4 *>(row + loc.col) = lo;
         *reinterpret_cast<uint4 *>(row + loc.col + 16) = hi;
       } else {
-        store32_bytes(row + loc.col, loc.remain, lo, hi);
+        store32_any(row + loc.col, loc.remain, lo, hi);
       }
     });
   }

@@ -141,18 +141,16 @@ int launch_gf8(const ApplyArgs &a, const PtrTable *pt, bool verify, cudaStream_t
 // length (a packed odd length would put most rows on the byte paths).
 static size_t pitch16(size_t len) { return (len + 15) & ~size_t(15); }
 
-// Encode route for a shape, length and row alignment (`align`: the OR of the rows' base
-// addresses and strides): the compiled kernel where the shape has one and the shard
-// holds at least two 32-column groups, else the matrix kernel. Under the automatic
-// route the generator kernels also need 16-byte aligned rows: on unaligned rows their
-// per-byte staging makes them 0.5-0.7x the matrix kernel (measured on B200 for (10,10),
-// (10,4), (20,12) at 1..256 stripes), while the FFT kernels stay about 3x ahead.
-bool use_fft8(const rs8_codec *c, size_t len, uintptr_t align) {
+// Encode route for a shape and length: the compiled kernel where the shape has one and
+// the shard holds at least two 32-column groups, else the matrix kernel. Row alignment
+// does not change the route: with the aligned-window staging of unaligned rows the
+// generator kernels measured 1.1-2.5x the matrix kernel there too ((10,10), (20,12) at
+// 1..256 stripes; (10,4) at 4 KiB 0.73-1.4x), and the FFT kernels stay further ahead.
+bool use_fft8(const rs8_codec *c, size_t len) {
   int r = c->route.load();
   if (r == 1 || !c->gen->fft) return false;
   if (r == 2) return true;
-  if (len < 64) return false;
-  return !(c->gen->fft->gen && (align & 15));
+  return len >= 64;
 }
 
 // The compiled kernel rereads all k data rows and does an encode's work, about (k+m)
@@ -172,9 +170,7 @@ int encode8_strided(rs8_codec *c, const uint8_t *in_base, uint64_t in_row, uint6
                            uint8_t *out_base, uint64_t out_row, uint64_t out_stripe, size_t n_stripes,
                            size_t len, cudaStream_t st) {
   const Gen8 &g = *c->gen;
-  const uintptr_t align = reinterpret_cast<uintptr_t>(in_base) | reinterpret_cast<uintptr_t>(out_base) | in_row |
-                          in_stripe | out_row | out_stripe;
-  if (use_fft8(c, len, align))
+  if (use_fft8(c, len))
     return launch_fft8(*g.fft, in_base, in_row, in_stripe, out_base, out_row, out_stripe,
                        (uint32_t)n_stripes, len, st);
   ApplyArgs a{};
@@ -284,10 +280,7 @@ static int reconstruct8(const Gen8 &g, PlanCache *cache, const Plan *fixed, Exec
     // rebuilds the missing data rows (its plan's leading rows), then the compiled
     // kernel regenerates the missing parity from the whole data rows, storing only
     // those rows. Smaller calls are latency-bound and keep the single launch.
-    uintptr_t align = 0;
-    for (size_t i = 0; i < n; i++) align |= reinterpret_cast<uintptr_t>(shards[i]);
     const bool split = !data_only && len >= 64 && (route == 2 || len >= ((size_t)64 << 10)) &&
-                       (route == 2 || !(g.fft && g.fft->gen && (align & 15))) &&
                        regen_parity_pays(g, plan->missing_parity.size(), route);
     const size_t mrows = split ? plan->missing_data.size() : rows;
     if (mrows) {
@@ -751,9 +744,7 @@ int rs8_encode_dev(rs8_t *c, uint8_t *const *d_shards, size_t n_shards, size_t l
   RSB_TRY(check_equal_lengths(n, len));
   RSB_CU(cudaSetDevice(g.device));
   cudaStream_t st = (cudaStream_t)stream;
-  uintptr_t align = 0;
-  for (size_t i = 0; i < n; i++) align |= reinterpret_cast<uintptr_t>(d_shards[i]);
-  if (use_fft8(c, len, align)) return launch_fft8_ptrs(*g.fft, d_shards, len, st);
+  if (use_fft8(c, len)) return launch_fft8_ptrs(*g.fft, d_shards, len, st);
   PtrTable pt;
   for (size_t i = 0; i < g.k; i++) pt.in[i] = d_shards[i];
   for (size_t j = 0; j < g.m; j++) pt.out[j] = d_shards[g.k + j];
@@ -853,7 +844,7 @@ int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, s
   // (missing data + missing parity) x k, where that pays (regen_parity_pays). Measured
   // on B200 (RS(32,32), 1..m erasures per stripe, both forms timed in one process):
   // +10% at 4 KiB shards, +21% at 16 KiB, +28% at 64 KiB.
-  const bool split = !data_only && use_fft8(c, row_len, reinterpret_cast<uintptr_t>(d_rows) | stripe_stride | row_len);
+  const bool split = !data_only && use_fft8(c, row_len);
   // Host side: per-stripe survivors and targets.
   std::vector<uint16_t> surv(n_stripes * k), targ(n_stripes * g.m), ntarg(n_stripes);
   std::vector<int> status(n_stripes, 0);
@@ -959,7 +950,8 @@ int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, s
                          st));
   const uint64_t groups = items.back().group_begin + (row_len + 31) / 32;
   return launch_fft8_items(*g.fft, reinterpret_cast<const FftItem *>(base + o_items), (uint32_t)items.size(), groups,
-                           st, reinterpret_cast<const uint32_t *>(base + o_masks));
+                           st, reinterpret_cast<const uint32_t *>(base + o_masks),
+                           ((reinterpret_cast<uintptr_t>(d_rows) | stripe_stride | row_len) & 15) != 0);
 }
 
 // ------------------------------- gf slices -----------------------------------

@@ -36,6 +36,7 @@ struct rs_batch {
     uint32_t n;
     uint64_t groups;
     const uint32_t *masks;  // parity rows to store per item; null: every row
+    bool unaligned;         // some item's rows are not 16-byte aligned
   };
   std::vector<FftLaunch> ffts;    // encodes
   std::vector<FftLaunch> regens;  // missing parity of reconstructs, after the data rows
@@ -56,13 +57,14 @@ struct rs_batch {
 namespace rsb {
 
 static int batch_enqueue(rs_batch *b, cudaStream_t st) {
-  for (const auto &f : b->ffts) RSB_TRY(launch_fft8_items(*f.shape, f.items, f.n, f.groups, st));
+  for (const auto &f : b->ffts) RSB_TRY(launch_fft8_items(*f.shape, f.items, f.n, f.groups, st, nullptr, f.unaligned));
   if (b->n_ragged) {
     gf8_ragged_kernel<8><<<(unsigned)b->ragged_blocks, kThreads, b->ragged_smem, st>>>(b->ragged, b->n_ragged);
     g_launches++;
     RSB_CU(cudaGetLastError());
   }
-  for (const auto &f : b->regens) RSB_TRY(launch_fft8_items(*f.shape, f.items, f.n, f.groups, st, f.masks));
+  for (const auto &f : b->regens)
+    RSB_TRY(launch_fft8_items(*f.shape, f.items, f.n, f.groups, st, f.masks, f.unaligned));
   return RS_OK;
 }
 
@@ -132,8 +134,7 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     const size_t n = g.k + g.m;
     if (it.op == RS_BATCH_ENCODE) {
       b->bytes += n * it.row_len;
-      if (!(flags & RS_BATCH_MATRIX_ONLY) &&
-          use_fft8(it.codec, it.row_len, reinterpret_cast<uintptr_t>(it.d_rows) | it.row_stride))
+      if (!(flags & RS_BATCH_MATRIX_ONLY) && use_fft8(it.codec, it.row_len))
         fft_groups[g.fft].push_back(i);
       else
         matrix_encodes.push_back(i);
@@ -166,8 +167,7 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     // kernel after the data rows are whole, storing only the missing rows, where that
     // beats the matrix route (regen_parity_pays).
     const bool regen = it.op == RS_BATCH_RECONSTRUCT && !(flags & RS_BATCH_MATRIX_ONLY) &&
-                       use_fft8(it.codec, it.row_len, reinterpret_cast<uintptr_t>(it.d_rows) | it.row_stride) &&
-                       regen_parity_pays(g, mp.size(), it.codec->route.load());
+                       use_fft8(it.codec, it.row_len) && regen_parity_pays(g, mp.size(), it.codec->route.load());
     rc.targets = md;
     if (it.op == RS_BATCH_RECONSTRUCT && !regen) rc.targets.insert(rc.targets.end(), mp.begin(), mp.end());
     if (regen) regen_groups[g.fft].push_back({i, mp, md.empty()});
@@ -263,14 +263,17 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     const FftShape *shape;
     size_t off, n;
     uint64_t groups;
+    bool unaligned;
   };
   std::vector<FftGroupOff> fgo;
   std::vector<std::vector<FftItem>> fft_host;
   for (auto &kv : fft_groups) {
     std::vector<FftItem> v;
     uint64_t g0 = 0;
+    uintptr_t align = 0;
     for (size_t i : kv.second) {
       const rs_batch_item &it = items[i];
+      align |= reinterpret_cast<uintptr_t>(it.d_rows) | it.row_stride;
       FftItem f{};
       f.in_base = it.d_rows;
       f.out_base = it.d_rows + (size_t)kv.first->k * it.row_stride;
@@ -280,7 +283,7 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
       g0 += (it.row_len + 31) / 32;
       v.push_back(f);
     }
-    fgo.push_back({kv.first, ar.put(v.data(), v.size() * sizeof(FftItem)), v.size(), g0});
+    fgo.push_back({kv.first, ar.put(v.data(), v.size() * sizeof(FftItem)), v.size(), g0, (align & 15) != 0});
     b->fft_items += v.size();
     fft_host.push_back(std::move(v));
   }
@@ -288,15 +291,18 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     const FftShape *shape;
     size_t off, mask_off, n;
     uint64_t groups;
+    bool unaligned;
   };
   std::vector<RegenOff> rgo;
   for (auto &kv : regen_groups) {
     std::vector<FftItem> v;
     std::vector<uint32_t> masks(4 * kv.second.size(), 0u);
     uint64_t g0 = 0;
+    uintptr_t align = 0;
     for (size_t p = 0; p < kv.second.size(); p++) {
       const Regen &rg = kv.second[p];
       const rs_batch_item &it = items[rg.item];
+      align |= reinterpret_cast<uintptr_t>(it.d_rows) | it.row_stride;
       FftItem f{};
       f.in_base = it.d_rows;
       f.out_base = it.d_rows + (size_t)kv.first->k * it.row_stride;
@@ -309,7 +315,8 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
       if (rg.only) b->fft_items++;
     }
     size_t off = ar.put(v.data(), v.size() * sizeof(FftItem));
-    rgo.push_back({kv.first, off, ar.put(masks.data(), masks.size() * sizeof(uint32_t)), v.size(), g0});
+    rgo.push_back({kv.first, off, ar.put(masks.data(), masks.size() * sizeof(uint32_t)), v.size(), g0,
+                   (align & 15) != 0});
   }
 
   // ---- allocate, patch device pointers, upload ----
@@ -357,10 +364,10 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
 
   for (auto &f : fgo)
     b->ffts.push_back({f.shape, reinterpret_cast<const FftItem *>(base + f.off), (uint32_t)f.n,
-                       f.groups, nullptr});
+                       f.groups, nullptr, f.unaligned});
   for (auto &f : rgo)
     b->regens.push_back({f.shape, reinterpret_cast<const FftItem *>(base + f.off), (uint32_t)f.n, f.groups,
-                         reinterpret_cast<const uint32_t *>(base + f.mask_off)});
+                         reinterpret_cast<const uint32_t *>(base + f.mask_off), f.unaligned});
   b->ragged = reinterpret_cast<const RaggedItem *>(base + ragged_off);
   b->n_ragged = (uint32_t)ragged.size();
   b->ragged_blocks = blocks;

@@ -566,8 +566,10 @@ static int enqueue_gf8(rs_server *s, Group &g, cudaStream_t st) {
   for (auto &kv : ffts) {
     const auto &v = kv.second;
     uint64_t groups = v.back().group_begin + (v.back().len + 31) / 32;
+    uintptr_t align = 0;
+    for (const FftItem &f : v) align |= reinterpret_cast<uintptr_t>(f.in_base) | f.row_stride;
     RSB_TRY(launch_fft8_items(*kv.first, reinterpret_cast<const FftItem *>(gd + off),
-                              (uint32_t)v.size(), groups, st));
+                              (uint32_t)v.size(), groups, st, nullptr, (align & 15) != 0));
     g.launches++;
     off = up256(off + v.size() * sizeof(FftItem));
   }
@@ -729,10 +731,7 @@ static void launch_group(rs_server *s, Group *g) {
 static bool route_fft(const rs_server *s, const rs_request &r) {
   const FftShape *sh = find_fft_shape(r.data_shards, r.parity_shards);
   if (!sh || r.op != RS_BATCH_ENCODE) return false;
-  // Generator shapes: no per-size hints; rows must be 16-byte aligned (host rows are
-  // staged at row_len apart in the arena).
-  if (sh->gen)
-    return r.row_len >= 64 && !((r.row_len | (r.rows_on_host ? 0 : reinterpret_cast<uintptr_t>(r.rows))) & 15);
+  if (sh->gen) return r.row_len >= 64;  // no per-size hints for generator shapes
   int kl = 0;
   while ((1 << (kl + 1)) <= sh->k) kl++;
   int bl = 0;

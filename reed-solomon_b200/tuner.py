@@ -256,19 +256,19 @@ class CostModel:
 
 DEFAULT_FFT = {2: (0, 0), 4: (0, 1), 8: (0, 1), 16: (0, 1), 32: (0, 3), 64: (0, 3), 128: (1, 3)}
 # The library's automatic choice on rows that are not 16-byte aligned (K >= 16).
-UNALIGNED_FFT = {16: (1, 2), 32: (1, 2), 64: (1, 1), 128: (1, 1)}
+UNALIGNED_FFT = {16: (1, 1), 32: (1, 1), 64: (1, 1), 128: (1, 1)}
 
 
 def default_choice(workloads, T):
     """The method without the model: the library's default route and tile (the FFT
-    kernel with its per-K default launch shape, or the generator kernel on 16-byte
-    aligned rows, where the shape has one, else matrix tile 0)."""
+    kernel with its launch shape for the rows' alignment, or the generator kernel,
+    where the shape has one, else matrix tile 0)."""
     out = np.zeros(len(workloads), np.int64)
     for i, w in enumerate(workloads):
         if applicable(w, ("fft", (0, 0))) and np.isfinite(T[i, 4]):
             aligned = w.shard_bytes % 16 == 0  # rows packed shard_bytes apart
             out[i] = CONFIGS.index(("fft", DEFAULT_FFT[w.k] if aligned or w.k < 16 else UNALIGNED_FFT[w.k]))
-        elif applicable(w, ("gen", 0)) and w.shard_bytes % 16 == 0:  # rows packed shard_bytes apart
+        elif applicable(w, ("gen", 0)):
             out[i] = CONFIGS.index(("gen", 0))
     return out
 

@@ -100,7 +100,7 @@ def stripes_sweep(shapes=((32, 32), (16, 16)), sizes=(4096, 65536, 1 << 20), n_s
 
 # ---- mixed batch: 10,000 stripes of nine shapes, 25% reconstruct ----
 
-def mixed_batch(n=10000, seed=3, reps=5):
+def mixed_batch(n=10000, seed=3, reps=5, packed=False):
     """Batched+tuned (one graph: one compiled-kernel launch per FFT or generator shape + one
     ragged matrix launch) against
     the plain path (one matrix-kernel call per stripe; reconstructs build their decode
@@ -117,8 +117,9 @@ def mixed_batch(n=10000, seed=3, reps=5):
         op = RECONSTRUCT if rng.random() < 0.25 else ENCODE
         present = _erasures(rng, k + m, m) if op == RECONSTRUCT else None
         # Each shard starts on a 16-byte boundary, as separately allocated shard buffers
-        # do; its length S is any integer (most are not multiples of 16 or 64).
-        stride = (S + 15) & ~15
+        # do; its length S is any integer (most are not multiples of 16 or 64). With
+        # `packed` the rows lie back to back at S apart, so most rows start unaligned.
+        stride = S if packed else (S + 15) & ~15
         specs.append((k, m, S, stride, op, present, off))
         off += ((k + m) * stride + 255) & ~255
     pool = torch.empty(off, dtype=torch.uint8, device="cuda")

@@ -235,3 +235,27 @@ def test_encode_dev_unaligned_pointers(gpu, O, k, m):
         torch.cuda.synchronize()
         got = np.array([b.cpu().numpy() for b in bufs[k:]])
         assert np.array_equal(got, O.encode8(k, m, host)), route
+
+
+@pytest.mark.parametrize("k,m", [(32, 32), (16, 16), (10, 10), (10, 4), (64, 64), (128, 128), (20, 12)])
+def test_encode_batch_packed_unaligned_rows(gpu, O, k, m):
+    """Rows packed back to back at odd lengths start at every offset mod 16, so the
+    compiled kernels' unaligned paths all run (a row's first group by bytes, interior
+    groups through the aligned 48-byte window, the tail by bytes, stores split at the
+    group's edges); the bytes equal the oracle's on every route."""
+    import torch
+
+    rng = np.random.default_rng(k * 7 + m)
+    stripes = 3
+    for length in (33, 63, 65, 95, 97, 100, 129, 987, 4099):
+        data = rng.integers(0, 256, size=(stripes, k, length), dtype=np.uint8)
+        want = np.stack([O.encode8(k, m, data[s]) for s in range(stripes)])
+        d = torch.from_numpy(data.reshape(-1)).cuda()
+        for route in ("fft", "auto", "matrix"):
+            rs = gpu.ReedSolomon(k, m)
+            rs.set_route(route)
+            par = torch.full((stripes * m * length,), 0xA5, dtype=torch.uint8, device="cuda")
+            rs.encode_batch_dev(d, par, length, stripes)
+            torch.cuda.synchronize()
+            got = par.cpu().numpy().reshape(stripes, m, length)
+            assert np.array_equal(got, want), (k, m, length, route)
