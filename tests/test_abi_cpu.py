@@ -115,3 +115,27 @@ def test_decode_rows_match_oracle(rsb, O, field, k, m):
 def test_decode_rows_too_few_present(rsb):
     st, _ = _decode_rows(rsb, 8, 4, 2, [1, 1, 1, 0, 0, 0])
     assert st == 10
+
+
+def test_fft_tuning_hooks_and_automatic_choice(rsb):
+    """rs_set_fft_variant / rs_set_fft_lanes return the previous value, reject shapes
+    without an FFT kernel (generator shapes included) and out-of-range values, and -1
+    restores the automatic choice (host state only, no device needed)."""
+    L = rsb.load()
+    n = L.rs_fft_variant_count()
+    assert n >= 4
+    base = L.rs_set_fft_variant(32, 2)
+    assert 0 <= base < n
+    assert L.rs_set_fft_variant(32, 1) == 2
+    assert L.rs_set_fft_variant(32, -1) == 1
+    assert L.rs_set_fft_variant(32, -1) == base  # back to the tuned default
+    assert L.rs_set_fft_variant(32, n) == -1
+    assert L.rs_set_fft_variant(32, -2) == -1
+    assert L.rs_set_fft_variant(10, 0) == -1  # (10,10) is a generator shape
+    assert L.rs_set_fft_variant(24, 0) == -1  # no compiled kernel
+    wide = L.rs_set_fft_lanes(128, 0)
+    assert wide in (0, 1)
+    assert L.rs_set_fft_lanes(128, -1) == 0
+    assert L.rs_set_fft_lanes(128, -1) == wide
+    assert L.rs_set_fft_lanes(128, 2) == -1
+    assert L.rs_set_fft_lanes(14, 0) == -1
