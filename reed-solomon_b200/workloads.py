@@ -304,7 +304,7 @@ def poisson_requests(count, rate, seed):
     return out
 
 
-def serve_poisson(count=400, rate=50000.0, seed=5, arena_bytes=4 << 30, slots=64, streams=8, max_batch=64,
+def serve_poisson(count=400, rate=50000.0, seed=5, arena_bytes=4 << 30, slots=64, streams=16, max_batch=64,
                   lookahead=64, route_hints=None):
     """Submits `count` requests at their Poisson arrival times (device-resident stripes
     carved from one synthetic pool; overlapping stripes share bytes, which changes no
