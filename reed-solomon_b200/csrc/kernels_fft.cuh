@@ -637,7 +637,13 @@ static __device__ __noinline__ void store32_any(uint8_t *p, uint64_t remain, uin
 // (j << W) | q. The next round's 32 bytes per shard are copied into shared memory with
 // cp.async while the current round computes. Every lane runs every round (on zeros
 // past the end) so each shuffle sees the full warp and every barrier the full CTA.
-template <int K, int W, bool PTRS, int THREADS, int CTAS, bool SYNC>
+// UNAL: the instantiation for launches whose rows are not 16-byte aligned (chosen on the
+// host). Its lanes on slow rounds park their parity registers in the staging slots and
+// store them from one rolled loop, issuing the next round's copies after it: the
+// unrolled body then holds no out-of-line calls (+15% on 987-byte packed rows), which
+// the aligned instantiation keeps for its rare partial groups, since the extra live
+// state cost it 20% when shared.
+template <int K, int W, bool PTRS, int THREADS, int CTAS, bool SYNC, bool UNAL = false>
 __global__ void __launch_bounds__(THREADS, CTAS)
     fft_kk_kernel(const FftArgs a, const __grid_constant__ PtrTableT<PTRS> pt) {
   extern __shared__ __align__(16) uint8_t stage[];
@@ -734,6 +740,52 @@ __global__ void __launch_bounds__(THREADS, CTAS)
       uint4 hi = *reinterpret_cast<const uint4 *>(mine + j * St::kSlot + St::kHalf);
       r[j][0] = lo.x, r[j][1] = lo.y, r[j][2] = lo.z, r[j][3] = lo.w;
       r[j][4] = hi.x, r[j][5] = hi.y, r[j][6] = hi.z, r[j][7] = hi.w;
+    }
+    if constexpr (UNAL) {
+      const bool fast = live && whole(loc), early = fast || !live;
+      if (early && rd + 1 < rounds) prefetch(grp + stride);
+      phase_sync<SYNC>();
+      levels_up<K, W, 0, 0, SYNC>(r, q, qm);
+      levels_down<K, W, LG - 1, kB.beta, SYNC>(r, q, qm);
+      auto out_row = [&](int j) -> uint8_t * {
+        if constexpr (PTRS)
+          return pt.out[out_index(j)];
+        else
+          return loc.out0 + (uint64_t)out_index(j) * loc.out_rs;
+      };
+      if (fast) {
+#pragma unroll
+        for (int j = 0; j < S; j++) {
+          if (!fft_store_row(a, loc.unit, out_index(j))) continue;
+          uint8_t *row = out_row(j);
+          uint32_t w[8];
+#pragma unroll
+          for (int b = 0; b < 8; b++) w[b] = r[j][b];
+          bit_transpose(w);
+          *reinterpret_cast<uint4 *>(row + col) = make_uint4(w[0], w[1], w[2], w[3]);
+          *reinterpret_cast<uint4 *>(row + col + 16) = make_uint4(w[4], w[5], w[6], w[7]);
+        }
+      } else if (live) {
+#pragma unroll
+        for (int j = 0; j < S; j++) {
+          *reinterpret_cast<uint4 *>(mine + j * St::kSlot) = make_uint4(r[j][0], r[j][1], r[j][2], r[j][3]);
+          *reinterpret_cast<uint4 *>(mine + j * St::kSlot + St::kHalf) =
+              make_uint4(r[j][4], r[j][5], r[j][6], r[j][7]);
+        }
+#pragma unroll 1
+        for (int j = 0; j < S; j++) {
+          if (!fft_store_row(a, loc.unit, out_index(j))) continue;
+          const uint4 lo = *reinterpret_cast<const uint4 *>(mine + j * St::kSlot);
+          const uint4 hi = *reinterpret_cast<const uint4 *>(mine + j * St::kSlot + St::kHalf);
+          uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+          bit_transpose(w);
+          store32_any(out_row(j) + col, remain, make_uint4(w[0], w[1], w[2], w[3]),
+                      make_uint4(w[4], w[5], w[6], w[7]));
+        }
+      }
+      if (!early && rd + 1 < rounds) prefetch(grp + stride);
+      phase_sync<SYNC>();
+      continue;
     }
     if (rd + 1 < rounds) prefetch(grp + stride);
     phase_sync<SYNC>();
@@ -837,14 +889,14 @@ inline int &fft_lanes_choice(int K) {
   return c[l & 7];
 }
 
-template <int K, int W, bool PTRS, int V>
+template <int K, int W, bool PTRS, int V, bool UNAL = false>
 inline cudaError_t launch_fft_kwv(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
   constexpr FftVariant var = kFftVariants[V];
   uint64_t groups = a.items ? a.total_groups : (uint64_t)a.n_stripes * a.groups_per_stripe;
   uint64_t blocks = ((groups << W) + var.threads - 1) / var.threads;
   blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, (uint64_t)sm_count() * var.ctas));
   const int smem = (K >> W) * FftStage<var.threads>::kSlot;
-  auto kern = fft_kk_kernel<K, W, PTRS, var.threads, var.ctas, (bool)var.sync>;
+  auto kern = fft_kk_kernel<K, W, PTRS, var.threads, var.ctas, (bool)var.sync, UNAL>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -867,17 +919,15 @@ inline cudaError_t launch_fft_kw(const FftArgs &a, const PtrTableT<PTRS> &pt, cu
 
 template <int K, bool PTRS>
 inline cudaError_t launch_fft_k(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
-  int wide = fft_lanes_choice(K), variant = fft_variant_for(K);
-  if constexpr (!PTRS) {
+  const int wide = fft_lanes_choice(K), variant = fft_variant_for(K);
+  if constexpr (!PTRS && K >= 16) {
     const bool unaligned =
         a.items ? a.items_unaligned != 0
                 : ((reinterpret_cast<uintptr_t>(a.in_base) | reinterpret_cast<uintptr_t>(a.out_base) |
                     a.in_row_stride | a.in_stripe_stride | a.out_row_stride | a.out_stripe_stride) &
                    15u) != 0;
-    if (K >= 16 && unaligned && fft_shape_auto(K)) {
-      wide = 1;
-      variant = fft_unaligned_variant(K);
-    }
+    if (unaligned && fft_shape_auto(K))
+      return launch_fft_kwv<K, fft_w_hi(K), PTRS, fft_unaligned_variant(K), true>(a, pt, st);
   }
   if constexpr (fft_w_lo(K) == fft_w_hi(K)) {
     return launch_fft_kw<K, fft_w_lo(K), PTRS>(a, pt, st, variant);
