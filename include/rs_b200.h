@@ -329,9 +329,14 @@ int rs16_dec_reconstruct(rs16_dec_t *dec, uint8_t *const *shards, const size_t *
 int rs16_dec_clone(const rs16_dec_t *dec, rs16_dec_t **out);
 void rs16_dec_free(rs16_dec_t *dec);
 /* ReedSolomon16::encode_route, src/reedsolomon16.rs:335-346: "fft" (bitsliced tower
- * LCH transform, src/fft16.rs; k a power of two, any m, picked when its estimated work
- * is below the matrix kernel's) or "matrix". */
+ * LCH transform, src/fft16.rs; any k >= 2 and m, picked when its estimated work is
+ * below the matrix kernel's) or "matrix". This is the shape's route; on the automatic
+ * route an encode of few short stripes, where the transform's pass launches dominate,
+ * takes the matrix kernel when that is estimated to finish first. */
 const char *rs16_encode_route(const rs16_t *codec);
+/* The route an encode of n_stripes stripes of len-byte shards takes (introspection;
+ * no counterpart in the reference). */
+const char *rs16_encode_route_for(const rs16_t *codec, size_t len, size_t n_stripes);
 /* Forced-route test hook like rs8_set_route: 0 automatic, 1 matrix, 2 FFT (encode for
  * k >= 2; reconstruct plans built afterwards use the FFT erasure decoder). Both routes
  * give identical bytes. */

@@ -89,6 +89,7 @@ SIGNATURES = {
     "rs16_dec_clone": (_int, [_vp, _pp]),
     "rs16_dec_free": (None, [_vp]),
     "rs16_encode_route": (ctypes.c_char_p, [_vp]),
+    "rs16_encode_route_for": (ctypes.c_char_p, [_vp, _sz, _sz]),
     "rs16_set_route": (_int, [_vp, _int]),
     "rs16_encode_dev": (_int, [_vp, _pp, _sz, _sz, _vp]),
     "rs16_encode_batch_dev": (_int, [_vp, _vp, _sz, _vp, _sz, _sz, _sz, _vp]),

@@ -338,8 +338,12 @@ class ReedSolomon16(_Coder):
         _check(self._L.rs16_parity_matrix(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), out.size))
         return out.reshape(self._m, self._k)
 
-    def encode_route(self):
-        return self._L.rs16_encode_route(self._h).decode()
+    def encode_route(self, shard_len=None, n_stripes=1):
+        """The shape's route, or with shard_len the route of an encode of n_stripes
+        stripes of that shard length."""
+        if shard_len is None:
+            return self._L.rs16_encode_route(self._h).decode()
+        return self._L.rs16_encode_route_for(self._h, shard_len, n_stripes).decode()
 
     def set_route(self, route):
         """Test hook: "auto", "matrix" or "fft" (identical bytes on every route)."""

@@ -282,6 +282,22 @@ bool fft16_preferred(const Fft16Program &p) {
   return fft < matrix;
 }
 
+bool fft16_faster(const Fft16Program &p, size_t len, size_t n_stripes) {
+  auto passes = [](uint64_t size) {
+    int lg = 0;
+    while ((1ull << lg) < size) lg++;
+    return (uint64_t)(lg + 1) / 2;
+  };
+  uint64_t launches = 1 + (p.k < p.t ? 1 : 0);  // load (+ zeroing)
+  for (const Fft16Step &s : p.interp) launches += s.kind == Fft16Step::kTransform ? passes(s.size) : 1;
+  launches += p.evals.size() * (passes(p.t) + 1);  // transform + store per coset
+  const double groups = (double)n_stripes * (double)((len / 2 + 31) / 32);
+  const double t_fft = 5.2 * (double)launches + 6.5e-5 * (double)p.butterflies * groups;  // us
+  const double work = (double)p.k * (double)p.m * (double)len * (double)n_stripes;
+  const double t_matrix = 2.0 + std::max(1.07 * (double)p.k, 4.6e-7 * work);
+  return t_fft < t_matrix;
+}
+
 size_t fft16_scratch_bytes(const Fft16Program &p, size_t n_stripes, size_t len, size_t budget) {
   const uint64_t G = (len / 2 + 31) / 32, per_group = (uint64_t)p.regs() * 64;
   const uint64_t all = (uint64_t)n_stripes * G * per_group;

@@ -90,6 +90,15 @@ int fft16_decode_run(const Fft16Decode &d, const uint16_t *d_cols, uint8_t *scra
 bool fft16_build(size_t k, size_t m, Fft16Program &p);
 // Whether the FFT route's estimated work is below the tower matrix kernel's.
 bool fft16_preferred(const Fft16Program &p);
+// Whether the FFT route is expected to finish first for n_stripes stripes of len-byte
+// shards: about 5.2 us per launch plus 0.065 ns per butterfly and 32-symbol group,
+// against the matrix kernel's max(1.07 us per data shard, 0.46 ns per coefficient and
+// shard byte). Small calls are latency-bound (the FFT's chain of pass launches; the
+// matrix kernel's walk over the k data rows), large ones throughput-bound. Constants
+// fitted to B200 timings of both routes on 23 calls from (16,16) x 16 stripes of 2 KiB
+// to (4096,12288) and (2000,50) x 64 KiB; the fitted choice is within 3% of the faster
+// route on each of them.
+bool fft16_faster(const Fft16Program &p, size_t len, size_t n_stripes);
 // Scratch for one run: all stripes at once when that fits `budget`, else the largest
 // slice of one stripe's 32-symbol groups that does (at least one group).
 size_t fft16_scratch_bytes(const Fft16Program &p, size_t n_stripes, size_t len, size_t budget);

@@ -132,10 +132,13 @@ struct rs16_codec {
 };
 
 namespace rsb {
-static bool use_fft16(const rs16_codec *c) {
+// len / n_stripes: the call's shard length and stripe count; len 0: the shape alone
+// (its throughput estimate, as rs16_encode_route reports it).
+static bool use_fft16(const rs16_codec *c, size_t len = 0, size_t n_stripes = 1) {
   int r = c->route.load();
   if (r == 1 || !c->gen->fft) return false;
-  return r == 2 || fft16_preferred(*c->gen->fft);
+  if (r == 2) return true;
+  return len == 0 ? fft16_preferred(*c->gen->fft) : fft16_faster(*c->gen->fft, len, n_stripes);
 }
 }  // namespace rsb
 
@@ -396,6 +399,11 @@ const char *rs16_encode_route(const rs16_t *c) {
   return use_fft16(c) ? "fft" : "matrix";
 }
 
+const char *rs16_encode_route_for(const rs16_t *c, size_t len, size_t n_stripes) {
+  if (!c) return "invalid";
+  return use_fft16(c, len, std::max<size_t>(n_stripes, 1)) ? "fft" : "matrix";
+}
+
 int rs16_set_route(rs16_t *c, int route) {
   if (!c || route < 0 || route > 2) return RS_ERR_INVALID_ARGUMENT;
   c->route.store(route);
@@ -415,7 +423,7 @@ int rs16_encode(rs16_t *c, uint8_t *const *shards, size_t n_shards, size_t len) 
   RSB_TRY(ex.buf.ensure(n * len));
   for (size_t i = 0; i < g.k; i++)
     RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * len, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
-  if (use_fft16(c)) {
+  if (use_fft16(c, len)) {
     RSB_TRY(fft16_encode(g, ex.buf.ptr, len, 0, ex.buf.ptr + g.k * len, len, 0, 1, len, nullptr, ex.stream));
   } else {
     Apply16Args a{};
@@ -560,7 +568,7 @@ int rs16_encode_dev(rs16_t *c, uint8_t *const *d_shards, size_t n_shards, size_t
   RSB_TRY(check_len16(len));
   RSB_CU(cudaSetDevice(g.device));
   cudaStream_t st = (cudaStream_t)stream;
-  if (use_fft16(c)) {
+  if (use_fft16(c, len)) {
     void *d_table = nullptr;
     RSB_CU(scratch_alloc(&d_table, n * sizeof(void *), st));
     RSB_CU(cudaMemcpyAsync(d_table, d_shards, n * sizeof(void *), cudaMemcpyHostToDevice, st));
@@ -579,7 +587,7 @@ int rs16_encode_batch_dev(rs16_t *c, const uint8_t *d_data, size_t data_stride, 
   if (!d_data || !d_parity) return RS_ERR_INVALID_ARGUMENT;
   const Gen16 &g = *c->gen;
   RSB_CU(cudaSetDevice(g.device));
-  if (use_fft16(c))
+  if (use_fft16(c, row_len, n_stripes))
     return fft16_encode(g, d_data, row_len, data_stride, d_parity, row_len, parity_stride, n_stripes, row_len,
                         nullptr, (cudaStream_t)stream);
   Apply16Args a{};

@@ -928,7 +928,7 @@ int rs_server_submit(rs_server_t *s, const rs_request *reqs, size_t n, int *stat
       bool fits = need <= s->cfg.arena_bytes && up256(q->up_bytes) <= s->cfg.pinned_bytes;
       if (r.field == 16 && r.op == RS_BATCH_ENCODE) {
         auto p = std::make_shared<Fft16Program>();
-        if (fft16_build(r.data_shards, r.parity_shards, *p) && fft16_preferred(*p)) {
+        if (fft16_build(r.data_shards, r.parity_shards, *p) && fft16_faster(*p, r.row_len, 1)) {
           q->candidate = p;
           q->fft16 = p;
           q->scratch_budget = std::min<size_t>(kFft16ScratchBudget, s->cfg.arena_bytes / 8);

@@ -40,6 +40,7 @@ def test_fft_route_1024x1024(gpu, O):
     k = m = 1024
     rs = gpu.ReedSolomon16(k, m)
     assert rs.encode_route() == "fft"  # picked automatically at this shape
+    rs.set_route("fft")  # also for the short shards below
     data = _rand(k, 66, 1)  # short shards keep the oracle fast
     assert np.array_equal(_encode(rs, data, m), O.encode16(k, m, data))
     # 2 KiB shards, several stripes: FFT route == matrix route on the device.
@@ -61,6 +62,7 @@ def test_fft_route_4096x12288_cosets(gpu):
     k, m, S = 4096, 12288, 2048
     rs = gpu.ReedSolomon16(k, m)
     assert rs.encode_route() == "fft"
+    rs.set_route("fft")
     g = torch.Generator(device="cuda").manual_seed(9)
     d = torch.randint(0, 256, (1, k, S), dtype=torch.uint8, device="cuda", generator=g)
     p_fft = torch.empty((1, m, S), dtype=torch.uint8, device="cuda")
@@ -94,6 +96,7 @@ def test_fft_route_large_odd_k(gpu):
         S = 1026
         rs = gpu.ReedSolomon16(k, m)
         assert rs.encode_route() == "fft"
+        rs.set_route("fft")
         g = torch.Generator(device="cuda").manual_seed(k)
         d = torch.randint(0, 256, (2, k, S), dtype=torch.uint8, device="cuda", generator=g)
         p_fft = torch.empty((2, m, S), dtype=torch.uint8, device="cuda")
@@ -110,6 +113,24 @@ def test_route_choice(gpu):
     assert gpu.ReedSolomon16(2, 1).encode_route() == "matrix"
     assert gpu.ReedSolomon16(256, 256).encode_route() == "fft"
     assert gpu.ReedSolomon16(300, 500).encode_route() == "fft"
+
+
+def test_route_choice_per_call(gpu, O):
+    """On the automatic route a single short stripe of a small shape, where the
+    transform's pass launches dominate, takes the matrix kernel; many stripes or a
+    large shape take the FFT. Every route gives the oracle's bytes."""
+    rs = gpu.ReedSolomon16(32, 32)
+    assert rs.encode_route() == "fft"
+    assert rs.encode_route(2048, 1) == "matrix"
+    assert rs.encode_route(65536, 256) == "fft"
+    assert gpu.ReedSolomon16(512, 512).encode_route(2048, 1) == "fft"
+    rs.set_route("fft")
+    assert rs.encode_route(2048, 1) == "fft"
+    rs.set_route("matrix")
+    assert rs.encode_route(65536, 256) == "matrix"
+    rs.set_route("auto")
+    data = _rand(32, 2048, 11)
+    assert np.array_equal(_encode(rs, data, 32), O.encode16(32, 32, data))
 
 
 def _erase(full, erased):

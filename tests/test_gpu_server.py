@@ -170,11 +170,11 @@ def test_resident_tables_hit_and_evict(gpu, O):
     s = srv.stats()
     assert s["table_builds"] == 1 and s["table_hits"] == 5
     srv.close()
-    # Matrix-route shapes (few parity rows) whose generators (m*k*4 bytes, 32 KB each)
-    # cannot all stay resident in a 256 KiB arena force evictions.
+    # Matrix-route shapes (few data rows, short shards) whose generators (m*k*4 bytes,
+    # 32 KB each) cannot all stay resident in a 256 KiB arena force evictions.
     srv = gpu.Server(arena_bytes=256 << 10, slots=8)
     for i in range(12):
-        req, expect = _make(O, (16, ENC, 400 + i, 20, 64, False), seed=950 + i)
+        req, expect = _make(O, (16, ENC, 20, 400 + i, 64, False), seed=950 + i)
         req["tag"] = 100 + i
         srv.submit([req])
         srv.wait(1)
