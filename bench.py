@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--tuner-workloads", type=int, default=10000,
                     help="workloads the tuner times (about 5 applicable configurations each)")
     ap.add_argument("--requests", type=int, default=400, help="requests of the serve workload")
-    ap.add_argument("--rs16", default=None, help="rs16 workload: one shape K,M,STRIPES instead of both")
+    ap.add_argument("--rs16", default=None,
+                    help="rs16 workload: shapes K,M,STRIPES[,SHARD_BYTES] separated by '/' instead of both")
     ap.add_argument("--mixed-stripes", type=int, default=10000, help="stripes of the mixed workload")
     ap.add_argument("--mixed-packed", action="store_true",
                     help="mixed workload: rows packed back to back at their (odd) lengths")
@@ -354,8 +355,8 @@ def run_workload(args):
                     "value": res["batched_gbs"], "results": res}
         elif args.workload == "rs16":
             if args.rs16:
-                k16, m16, n16 = (int(x) for x in args.rs16.split(","))
-                res = workloads.rs16_shapes(shapes=((k16, m16, n16),))
+                res = workloads.rs16_shapes(shapes=[tuple(int(x) for x in sh.split(","))
+                                                    for sh in args.rs16.split("/")])
             else:
                 res = workloads.rs16_shapes()
             line = {"metric": "ReedSolomon16 encode/reconstruct GB/s", "unit": "GB/s", "results": res}

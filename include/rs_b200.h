@@ -332,7 +332,11 @@ void rs16_dec_free(rs16_dec_t *dec);
  * LCH transform, src/fft16.rs; any k >= 2 and m, picked when its estimated work is
  * below the matrix kernel's) or "matrix". This is the shape's route; on the automatic
  * route an encode of few short stripes, where the transform's pass launches dominate,
- * takes the matrix kernel when that is estimated to finish first. */
+ * takes the matrix kernel when that is estimated to finish first. "subfield": with
+ * k + m <= 256 every evaluation point, hence every coefficient, lies in GF(2^8), which
+ * scales the low and the high byte plane alike, so on the automatic route encode,
+ * verify and reconstruct run the GF(2^8) codec of the same shape over the shard bytes
+ * (after the tower's own argument checks; prepared decoders keep the tower kernels). */
 const char *rs16_encode_route(const rs16_t *codec);
 /* The route an encode of n_stripes stripes of len-byte shards takes (introspection;
  * no counterpart in the reference). */

@@ -129,9 +129,19 @@ struct rs16_codec {
   std::shared_ptr<PlanCache> plans;
   std::shared_ptr<Exec> exec;
   std::atomic<int> route{0};  // 0 automatic, 1 matrix, 2 FFT where available
+  // k + m <= 256: every evaluation point 0..k+m-1 lies in the GF(2^8) subfield
+  // (high byte 0), so every generator and decode coefficient does too, and a subfield
+  // constant c multiplies a tower symbol plane by plane: c(hi*y + lo) = (c*hi)y + c*lo.
+  // The tower code is then ReedSolomon(k, m) applied to every byte of the split-plane
+  // shards, and the automatic route runs it on the GF(2^8) codec's kernels.
+  rs8_t *sub = nullptr;
+  ~rs16_codec() { rs8_free(sub); }
 };
 
 namespace rsb {
+// The GF(2^8) codec that runs this shape on the automatic route, or null.
+static rs8_t *subfield(const rs16_codec *c) { return c->route.load() == 0 ? c->sub : nullptr; }
+
 // len / n_stripes: the call's shard length and stripe count; len 0: the shape alone
 // (its throughput estimate, as rs16_encode_route reports it).
 static bool use_fft16(const rs16_codec *c, size_t len = 0, size_t n_stripes = 1) {
@@ -260,7 +270,7 @@ static int fft16_reconstruct(const Gen16 &g, const Plan &plan, Exec &ex, uint8_t
 
 static int reconstruct16(const Gen16 &g, PlanCache *cache, const Plan *fixed, Exec &ex, int route,
                          uint8_t *const *shards, const size_t *lens, const uint8_t *present,
-                         size_t n_shards, bool data_only, bool dev, cudaStream_t st) {
+                         size_t n_shards, bool data_only, bool dev, cudaStream_t st, rs8_t *sub = nullptr) {
   size_t n = g.k + g.m;
   if (!shards || !lens || !present) return RS_ERR_INVALID_ARGUMENT;
   if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
@@ -271,6 +281,11 @@ static int reconstruct16(const Gen16 &g, PlanCache *cache, const Plan *fixed, Ex
   if (n_present == n) return RS_OK;
   if (!fixed && n_present < g.k) return RS_TOO_FEW_SHARDS_PRESENT;
   if (len == 0) return RS_TOO_FEW_SHARDS_PRESENT;
+  if (sub && !fixed) {  // the tower's checks passed; the subfield codec rebuilds
+    RSB_TRY(check_absent_buffers(lens, present, n, g.k, len, data_only));
+    return dev ? rs8_reconstruct_dev(sub, shards, lens, present, n, data_only ? 1 : 0, st)
+               : rs8_reconstruct(sub, shards, lens, present, n, data_only ? 1 : 0);
+  }
   std::shared_ptr<const Plan> hold;
   const Plan *plan = fixed;
   if (!plan) {
@@ -345,6 +360,7 @@ int rs16_new(size_t k, size_t m, rs16_t **out) {
   c->gen = gen;
   c->plans = std::make_shared<PlanCache>();
   int st = make_exec(dev, c->exec);
+  if (st == RS_OK && k + m <= 256) st = rs8_new(k, m, &c->sub);
   if (st) {
     delete c;
     return st;
@@ -362,6 +378,7 @@ int rs16_clone(const rs16_t *codec, rs16_t **out) {
   c->plans->copy_from(*codec->plans);
   c->route.store(codec->route.load());
   int st = make_exec(codec->gen->device, c->exec);
+  if (st == RS_OK && codec->sub) st = rs8_clone(codec->sub, &c->sub);
   if (st) {
     delete c;
     return st;
@@ -396,11 +413,13 @@ int rs16_parity_matrix(const rs16_t *c, uint16_t *out, size_t out_len) {
 
 const char *rs16_encode_route(const rs16_t *c) {
   if (!c) return "invalid";
+  if (subfield(c)) return "subfield";
   return use_fft16(c) ? "fft" : "matrix";
 }
 
 const char *rs16_encode_route_for(const rs16_t *c, size_t len, size_t n_stripes) {
   if (!c) return "invalid";
+  if (subfield(c)) return "subfield";
   return use_fft16(c, len, std::max<size_t>(n_stripes, 1)) ? "fft" : "matrix";
 }
 
@@ -417,6 +436,7 @@ int rs16_encode(rs16_t *c, uint8_t *const *shards, size_t n_shards, size_t len) 
   size_t n = g.k + g.m;
   if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
   RSB_TRY(check_len16(len));
+  if (rs8_t *sub = subfield(c)) return rs8_encode(sub, shards, n_shards, len);
   Exec &ex = *c->exec;
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
@@ -466,6 +486,7 @@ int rs16_verify(rs16_t *c, const uint8_t *const *shards, size_t n_shards, size_t
   size_t n = g.k + g.m;
   if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
   RSB_TRY(check_len16(len));
+  if (rs8_t *sub = subfield(c)) return rs8_verify(sub, shards, n_shards, len, ok);
   Exec &ex = *c->exec;
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
@@ -498,7 +519,7 @@ int rs16_reconstruct(rs16_t *c, uint8_t *const *shards, const size_t *lens, cons
                      size_t n_shards, int data_only) {
   if (!c) return RS_ERR_INVALID_ARGUMENT;
   return reconstruct16(*c->gen, c->plans.get(), nullptr, *c->exec, c->route.load(), shards, lens, present, n_shards,
-                       data_only != 0, false, nullptr);
+                       data_only != 0, false, nullptr, subfield(c));
 }
 
 // src/reedsolomon16.rs:544-565
@@ -566,6 +587,7 @@ int rs16_encode_dev(rs16_t *c, uint8_t *const *d_shards, size_t n_shards, size_t
   size_t n = g.k + g.m;
   if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
   RSB_TRY(check_len16(len));
+  if (rs8_t *sub = subfield(c)) return rs8_encode_dev(sub, d_shards, n_shards, len, stream);
   RSB_CU(cudaSetDevice(g.device));
   cudaStream_t st = (cudaStream_t)stream;
   if (use_fft16(c, len)) {
@@ -585,6 +607,8 @@ int rs16_encode_batch_dev(rs16_t *c, const uint8_t *d_data, size_t data_stride, 
   if (n_stripes == 0) return RS_OK;
   RSB_TRY(check_len16(row_len));
   if (!d_data || !d_parity) return RS_ERR_INVALID_ARGUMENT;
+  if (rs8_t *sub = subfield(c))
+    return rs8_encode_batch_dev(sub, d_data, data_stride, d_parity, parity_stride, n_stripes, row_len, stream);
   const Gen16 &g = *c->gen;
   RSB_CU(cudaSetDevice(g.device));
   if (use_fft16(c, row_len, n_stripes))
@@ -609,7 +633,7 @@ int rs16_reconstruct_dev(rs16_t *c, uint8_t *const *d_shards, const size_t *lens
                          size_t n_shards, int data_only, void *stream) {
   if (!c) return RS_ERR_INVALID_ARGUMENT;
   return reconstruct16(*c->gen, c->plans.get(), nullptr, *c->exec, c->route.load(), d_shards, lens, present, n_shards,
-                       data_only != 0, true, (cudaStream_t)stream);
+                       data_only != 0, true, (cudaStream_t)stream, subfield(c));
 }
 
 }  // extern "C"

@@ -917,10 +917,15 @@ int rs_server_submit(rs_server_t *s, const rs_request *reqs, size_t n, int *stat
     q->r = reqs[i];
     q->submit_ns = t;
     int st = validate(reqs[i], *q);
+    // A GF(2^16) request with k + m <= 256 has all its coefficients in the GF(2^8)
+    // subfield, which scales the two byte planes alike: after the tower's own checks it
+    // runs as the GF(2^8) request of its shape (and shares that shape's table and
+    // launch groups).
+    if (st == RS_OK && q->r.field == 16 && q->r.data_shards + q->r.parity_shards <= 256) q->r.field = 8;
     if (st == RS_OK) {
       // Largest working set it could ever need (building its table) must fit an empty
       // arena on at least one route.
-      const rs_request &r = reqs[i];
+      const rs_request &r = q->r;
       size_request(*q, true);
       size_t tb = (r.field == 8 || r.op == RS_BATCH_ENCODE) ? table_bytes(r.field, r.data_shards, r.parity_shards)
                                                              : 0;

@@ -191,11 +191,14 @@ def mixed_batch(n=10000, seed=3, reps=5, packed=False):
 # ---- ReedSolomon16: (1024,1024) and (4096,12288), 2 KiB shards ----
 
 def rs16_shapes(shapes=((1024, 1024, 64), (4096, 12288, 2)), S=2048, seed=4, reps=2):
+    """Each shape is (k, m, stripes) at S-byte shards, or (k, m, stripes, shard_bytes)."""
     import torch
 
     out = []
     rng = np.random.default_rng(seed)
-    for k, m, stripes in shapes:
+    for shape in shapes:
+        k, m, stripes = shape[:3]
+        S = shape[3] if len(shape) > 3 else S
         n = k + m
         rs = ReedSolomon16(k, m)
         g = torch.Generator(device="cuda").manual_seed(seed + k)
@@ -206,9 +209,13 @@ def rs16_shapes(shapes=((1024, 1024, 64), (4096, 12288, 2)), S=2048, seed=4, rep
             rs.encode_batch_dev(rows, rows[:, k:], S, stripes, data_stride=stride, parity_stride=stride)
 
         t_enc = _time(enc, reps)
-        route = rs.encode_route()
+        route = rs.encode_route(S, stripes)
         rs.set_route("matrix")
         t_mat = _time(enc, 1)
+        t_fft = None
+        if route != "fft" and k >= 2:  # the tower FFT, for comparison
+            rs.set_route("fft")
+            t_fft = _time(enc, 1)
         rs.set_route("auto")
         full = rows[0].clone()
         present = np.ones(n, np.uint8)
@@ -241,6 +248,7 @@ def rs16_shapes(shapes=((1024, 1024, 64), (4096, 12288, 2)), S=2048, seed=4, rep
         out.append({"k": k, "m": m, "shard_bytes": S, "stripes": stripes, "route": route,
                     "encode_gbs": stripes * n * S / t_enc / 1e9, "encode_ms_per_stripe": t_enc / stripes * 1e3,
                     "encode_matrix_gbs": stripes * n * S / t_mat / 1e9,
+                    "encode_tower_fft_gbs": stripes * n * S / t_fft / 1e9 if t_fft else None,
                     "reconstruct_m_erasures_gbs": (k + m) * S / t_rec / 1e9,
                     "reconstruct_ms": t_rec * 1e3, "reconstruct_cold_ms": t_cold * 1e3,
                     "reconstruct_bit_exact": exact and exact_cold})

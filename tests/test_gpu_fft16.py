@@ -109,17 +109,21 @@ def test_fft_route_large_odd_k(gpu):
 
 
 def test_route_choice(gpu):
-    assert gpu.ReedSolomon16(3, 2).encode_route() == "matrix"  # too small to pay off
-    assert gpu.ReedSolomon16(2, 1).encode_route() == "matrix"
+    assert gpu.ReedSolomon16(3, 2).encode_route() == "subfield"  # k + m <= 256
+    assert gpu.ReedSolomon16(200, 56).encode_route() == "subfield"
+    rs = gpu.ReedSolomon16(3, 2)
+    rs.set_route("matrix")
+    assert rs.encode_route() == "matrix"
     assert gpu.ReedSolomon16(256, 256).encode_route() == "fft"
     assert gpu.ReedSolomon16(300, 500).encode_route() == "fft"
 
 
 def test_route_choice_per_call(gpu, O):
-    """On the automatic route a single short stripe of a small shape, where the
-    transform's pass launches dominate, takes the matrix kernel; many stripes or a
-    large shape take the FFT. Every route gives the oracle's bytes."""
-    rs = gpu.ReedSolomon16(32, 32)
+    """On the automatic route a single short stripe, where the transform's pass
+    launches dominate, takes the matrix kernel; many stripes or a large shape take the
+    FFT. Every route gives the oracle's bytes."""
+    k, m = 64, 300
+    rs = gpu.ReedSolomon16(k, m)
     assert rs.encode_route() == "fft"
     assert rs.encode_route(2048, 1) == "matrix"
     assert rs.encode_route(65536, 256) == "fft"
@@ -129,8 +133,48 @@ def test_route_choice_per_call(gpu, O):
     rs.set_route("matrix")
     assert rs.encode_route(65536, 256) == "matrix"
     rs.set_route("auto")
-    data = _rand(32, 2048, 11)
-    assert np.array_equal(_encode(rs, data, 32), O.encode16(32, 32, data))
+    data = _rand(k, 2048, 11)
+    assert np.array_equal(_encode(rs, data, m), O.encode16(k, m, data))
+
+
+@pytest.mark.parametrize("k,m", [(7, 13), (2, 1), (32, 32), (100, 156), (3, 250)])
+def test_subfield_route(gpu, O, k, m):
+    """k + m <= 256: every coefficient lies in GF(2^8), so the automatic route runs
+    the GF(2^8) codec over both byte planes. Encode (host, device pointers, strided
+    batch), verify and reconstruct give the tower oracle's bytes and the tower
+    kernels' bytes; the tower's own checks (even, non-zero lengths) still apply."""
+    import torch
+
+    rs = gpu.ReedSolomon16(k, m)
+    assert rs.encode_route() == "subfield" and rs.encode_route(2048, 64) == "subfield"
+    for length in [2, 66, 130, 2048, 4098]:
+        data = _rand(k, length, 3 * k + m + length)
+        want = O.encode16(k, m, data)
+        assert np.array_equal(_encode(rs, data, m), want), (k, m, length)
+        full = [data[i].copy() for i in range(k)] + [want[j].copy() for j in range(m)]
+        assert rs.verify(full)
+        erased = [int(e) for e in np.random.default_rng(length).choice(k + m, size=m, replace=False)]
+        shards = _erase(full, erased)
+        rs.reconstruct([(s, i not in erased) for i, s in enumerate(shards)])
+        assert np.array_equal(np.array(shards), np.array(full)), (k, m, length, erased)
+    with pytest.raises(gpu.RsError):
+        _encode(rs, _rand(k, 65, 1), m)  # odd length: the tower's IncorrectShardSize
+    # Device-resident: strided batch and pointer table against the forced tower kernels.
+    S, stripes = 4098, 3
+    g = torch.Generator(device="cuda").manual_seed(k + m)
+    d = torch.randint(0, 256, (stripes, k, S), dtype=torch.uint8, device="cuda", generator=g)
+    p_sub = torch.empty((stripes, m, S), dtype=torch.uint8, device="cuda")
+    p_mat = torch.empty_like(p_sub)
+    rs.encode_batch_dev(d, p_sub, S, stripes)
+    rs.set_route("matrix")
+    rs.encode_batch_dev(d, p_mat, S, stripes)
+    rs.set_route("auto")
+    ptr_shards = [d[1, i].clone() for i in range(k)] + [torch.zeros(S, dtype=torch.uint8, device="cuda")
+                                                        for _ in range(m)]
+    rs.encode_dev(ptr_shards)
+    torch.cuda.synchronize()
+    assert torch.equal(p_sub, p_mat)
+    assert all(torch.equal(ptr_shards[k + j], p_mat[1, j]) for j in range(m))
 
 
 def _erase(full, erased):

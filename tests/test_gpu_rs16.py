@@ -27,9 +27,13 @@ def test_golden_wire_vector(gpu, golden):
     assert encode_gpu(rs, np.array(g["data"], np.uint8), g["m"]).tolist() == g["parity"]
 
 
+@pytest.mark.parametrize("route", ["auto", "matrix"])
 @pytest.mark.parametrize("k,m", [(4, 2), (7, 13), (10, 10), (17, 33), (1, 1), (300, 20)])
-def test_encode_matches_symbolwise(gpu, O, k, m):
+def test_encode_matches_symbolwise(gpu, O, k, m, route):
+    """The automatic route (the GF(2^8) codec for k + m <= 256) and the tower matrix
+    kernel both give the symbol-wise oracle's bytes."""
     rs = gpu.ReedSolomon16(k, m)
+    rs.set_route(route)
     assert np.array_equal(rs.parity_matrix(), O.build_matrix(16, k, k + m)[k:])
     for length in [2, 30, 32, 34, 62, 64, 66, 200, 2048, 4098]:
         if k * m * length > 40_000_000:
@@ -69,9 +73,11 @@ def test_odd_length_rejected(gpu):
     assert e.value.name == "EmptyShard"
 
 
+@pytest.mark.parametrize("route", ["auto", "matrix"])
 @pytest.mark.parametrize("k,m", [(4, 2), (17, 33), (10, 10), (100, 200)])
-def test_reconstruct_patterns(gpu, O, k, m):
+def test_reconstruct_patterns(gpu, O, k, m, route):
     rs = gpu.ReedSolomon16(k, m)
+    rs.set_route(route)
     total = k + m
     for length in [2, 34, 512]:
         data = rand(k, length, length + k)
