@@ -336,7 +336,9 @@ void rs16_dec_free(rs16_dec_t *dec);
  * k + m <= 256 every evaluation point, hence every coefficient, lies in GF(2^8), which
  * scales the low and the high byte plane alike, so on the automatic route encode,
  * verify and reconstruct run the GF(2^8) codec of the same shape over the shard bytes
- * (after the tower's own argument checks; prepared decoders keep the tower kernels). */
+ * (after the tower's own argument checks; prepared decoders keep the tower kernels),
+ * except an encode that would run the GF(2^8) matrix kernel where the tower FFT is
+ * estimated faster (rs16_encode_route_for then reports "fft"). */
 const char *rs16_encode_route(const rs16_t *codec);
 /* The route an encode of n_stripes stripes of len-byte shards takes (introspection;
  * no counterpart in the reference). */

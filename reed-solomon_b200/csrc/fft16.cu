@@ -282,7 +282,7 @@ bool fft16_preferred(const Fft16Program &p) {
   return fft < matrix;
 }
 
-bool fft16_faster(const Fft16Program &p, size_t len, size_t n_stripes) {
+static double fft16_time_us(const Fft16Program &p, size_t len, size_t n_stripes) {
   auto passes = [](uint64_t size) {
     int lg = 0;
     while ((1ull << lg) < size) lg++;
@@ -292,10 +292,19 @@ bool fft16_faster(const Fft16Program &p, size_t len, size_t n_stripes) {
   for (const Fft16Step &s : p.interp) launches += s.kind == Fft16Step::kTransform ? passes(s.size) : 1;
   launches += p.evals.size() * (passes(p.t) + 1);  // transform + store per coset
   const double groups = (double)n_stripes * (double)((len / 2 + 31) / 32);
-  const double t_fft = 5.2 * (double)launches + 6.5e-5 * (double)p.butterflies * groups;  // us
+  return 5.2 * (double)launches + 6.5e-5 * (double)p.butterflies * groups;
+}
+
+bool fft16_faster(const Fft16Program &p, size_t len, size_t n_stripes) {
   const double work = (double)p.k * (double)p.m * (double)len * (double)n_stripes;
   const double t_matrix = 2.0 + std::max(1.07 * (double)p.k, 4.6e-7 * work);
-  return t_fft < t_matrix;
+  return fft16_time_us(p, len, n_stripes) < t_matrix;
+}
+
+bool fft16_faster_than_gf8_matrix(const Fft16Program &p, size_t len, size_t n_stripes) {
+  const double work = (double)p.k * (double)p.m * (double)len * (double)n_stripes;
+  const double t_matrix = 2.0 + std::max(0.61 * (double)p.k, 2.0e-7 * work);
+  return fft16_time_us(p, len, n_stripes) < t_matrix;
 }
 
 size_t fft16_scratch_bytes(const Fft16Program &p, size_t n_stripes, size_t len, size_t budget) {

@@ -99,6 +99,12 @@ bool fft16_preferred(const Fft16Program &p);
 // to (4096,12288) and (2000,50) x 64 KiB; the fitted choice is within 3% of the faster
 // route on each of them.
 bool fft16_faster(const Fft16Program &p, size_t len, size_t n_stripes);
+// The same against the GF(2^8) matrix kernel, which a shape with k + m <= 256 can use
+// instead (every coefficient in the subfield): about 0.2 ns per coefficient and shard
+// byte on B200 (RS(32,32) at 343 GB/s, (100,156) x 64 x 16 KiB at 81 GB/s), the
+// per-shard latency term scaled by the same 0.57 as the (100,156) throughput against
+// the tower kernel. Measured there: tower FFT 123 GB/s, the GF(2^8) matrix kernel 81.
+bool fft16_faster_than_gf8_matrix(const Fft16Program &p, size_t len, size_t n_stripes);
 // Scratch for one run: all stripes at once when that fits `budget`, else the largest
 // slice of one stripe's 32-symbol groups that does (at least one group).
 size_t fft16_scratch_bytes(const Fft16Program &p, size_t n_stripes, size_t len, size_t budget);

@@ -142,6 +142,16 @@ namespace rsb {
 // The GF(2^8) codec that runs this shape on the automatic route, or null.
 static rs8_t *subfield(const rs16_codec *c) { return c->route.load() == 0 ? c->sub : nullptr; }
 
+// Whether an encode of n_stripes stripes of len-byte shards runs on the subfield codec:
+// always where that codec has a compiled kernel for the call (FFT or generator shapes);
+// on its matrix kernel only when the tower FFT is not estimated to finish first.
+static bool subfield_encode(const rs16_codec *c, size_t len, size_t n_stripes) {
+  rs8_t *sub = subfield(c);
+  if (!sub) return false;
+  if (std::strcmp(rs8_encode_route(sub, len), "matrix") != 0 || !c->gen->fft) return true;
+  return !fft16_faster_than_gf8_matrix(*c->gen->fft, len, std::max<size_t>(n_stripes, 1));
+}
+
 // len / n_stripes: the call's shard length and stripe count; len 0: the shape alone
 // (its throughput estimate, as rs16_encode_route reports it).
 static bool use_fft16(const rs16_codec *c, size_t len = 0, size_t n_stripes = 1) {
@@ -419,7 +429,7 @@ const char *rs16_encode_route(const rs16_t *c) {
 
 const char *rs16_encode_route_for(const rs16_t *c, size_t len, size_t n_stripes) {
   if (!c) return "invalid";
-  if (subfield(c)) return "subfield";
+  if (subfield_encode(c, len, n_stripes)) return "subfield";
   return use_fft16(c, len, std::max<size_t>(n_stripes, 1)) ? "fft" : "matrix";
 }
 
@@ -436,7 +446,7 @@ int rs16_encode(rs16_t *c, uint8_t *const *shards, size_t n_shards, size_t len) 
   size_t n = g.k + g.m;
   if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
   RSB_TRY(check_len16(len));
-  if (rs8_t *sub = subfield(c)) return rs8_encode(sub, shards, n_shards, len);
+  if (subfield_encode(c, len, 1)) return rs8_encode(c->sub, shards, n_shards, len);
   Exec &ex = *c->exec;
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
@@ -587,7 +597,7 @@ int rs16_encode_dev(rs16_t *c, uint8_t *const *d_shards, size_t n_shards, size_t
   size_t n = g.k + g.m;
   if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
   RSB_TRY(check_len16(len));
-  if (rs8_t *sub = subfield(c)) return rs8_encode_dev(sub, d_shards, n_shards, len, stream);
+  if (subfield_encode(c, len, 1)) return rs8_encode_dev(c->sub, d_shards, n_shards, len, stream);
   RSB_CU(cudaSetDevice(g.device));
   cudaStream_t st = (cudaStream_t)stream;
   if (use_fft16(c, len)) {
@@ -607,8 +617,8 @@ int rs16_encode_batch_dev(rs16_t *c, const uint8_t *d_data, size_t data_stride, 
   if (n_stripes == 0) return RS_OK;
   RSB_TRY(check_len16(row_len));
   if (!d_data || !d_parity) return RS_ERR_INVALID_ARGUMENT;
-  if (rs8_t *sub = subfield(c))
-    return rs8_encode_batch_dev(sub, d_data, data_stride, d_parity, parity_stride, n_stripes, row_len, stream);
+  if (subfield_encode(c, row_len, n_stripes))
+    return rs8_encode_batch_dev(c->sub, d_data, data_stride, d_parity, parity_stride, n_stripes, row_len, stream);
   const Gen16 &g = *c->gen;
   RSB_CU(cudaSetDevice(g.device));
   if (use_fft16(c, row_len, n_stripes))

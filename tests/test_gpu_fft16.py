@@ -146,7 +146,13 @@ def test_subfield_route(gpu, O, k, m):
     import torch
 
     rs = gpu.ReedSolomon16(k, m)
-    assert rs.encode_route() == "subfield" and rs.encode_route(2048, 64) == "subfield"
+    assert rs.encode_route() == "subfield" and rs.encode_route(2048, 1) == "subfield"
+    if (k, m) == (100, 156):
+        # No compiled GF(2^8) kernel for this shape: a large batch is estimated faster
+        # on the tower FFT than on the GF(2^8) matrix kernel.
+        assert rs.encode_route(16384, 64) == "fft"
+    else:
+        assert rs.encode_route(2048, 64) == "subfield"
     for length in [2, 66, 130, 2048, 4098]:
         data = _rand(k, length, 3 * k + m + length)
         want = O.encode16(k, m, data)
@@ -175,6 +181,25 @@ def test_subfield_route(gpu, O, k, m):
     torch.cuda.synchronize()
     assert torch.equal(p_sub, p_mat)
     assert all(torch.equal(ptr_shards[k + j], p_mat[1, j]) for j in range(m))
+
+
+def test_subfield_shape_batch_on_tower_fft(gpu):
+    """(100,156) x 64 stripes of 16 KiB takes the tower FFT on the automatic route; its
+    bytes equal the tower matrix kernel's."""
+    import torch
+
+    k, m, S, stripes = 100, 156, 16384, 64
+    rs = gpu.ReedSolomon16(k, m)
+    assert rs.encode_route(S, stripes) == "fft"
+    g = torch.Generator(device="cuda").manual_seed(17)
+    d = torch.randint(0, 256, (stripes, k, S), dtype=torch.uint8, device="cuda", generator=g)
+    p_auto = torch.empty((stripes, m, S), dtype=torch.uint8, device="cuda")
+    p_mat = torch.empty_like(p_auto)
+    rs.encode_batch_dev(d, p_auto, S, stripes)
+    rs.set_route("matrix")
+    rs.encode_batch_dev(d, p_mat, S, stripes)
+    torch.cuda.synchronize()
+    assert torch.equal(p_auto, p_mat)
 
 
 def _erase(full, erased):
