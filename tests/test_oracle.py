@@ -151,3 +151,28 @@ def test_oracle_reconstruct_round_trip(O, field):
             present[erased] = 0
             assert O.reconstruct(field, k, m, rows, present) == 0
             assert np.array_equal(rows, full)
+
+
+def test_tower_subfield_shapes_equal_gf8_code(O):
+    """With k + m <= 256 every evaluation point of the tower code has a zero high byte,
+    so its generator and decode coefficients lie in GF(2^8), which scales the low and
+    the high byte plane alike: the tower code is ReedSolomon(k, m) on the shard bytes.
+    The library's automatic tower route relies on this; the oracle shows it on encode,
+    the parity matrices and reconstruct. Past 256 shards it no longer holds."""
+    rng = np.random.default_rng(256)
+    for k, m in [(1, 1), (2, 1), (7, 13), (32, 32), (100, 156), (3, 250), (255, 1)]:
+        assert np.array_equal(O.build_matrix(16, k, k + m), O.build_matrix(8, k, k + m).astype(np.uint16))
+        data = rng.integers(0, 256, size=(k, 66), dtype=np.uint8)
+        par = O.encode16(k, m, data)
+        assert np.array_equal(par, O.encode8(k, m, data)), (k, m)
+        full = np.concatenate([data, par])
+        erased = rng.choice(k + m, size=m, replace=False)
+        present = np.ones(k + m, np.uint8)
+        present[erased] = 0
+        rows8, rows16 = full.copy(), full.copy()
+        rows8[erased] = 0
+        rows16[erased] = 0
+        assert O.reconstruct(8, k, m, rows8, present) == 0
+        assert O.reconstruct(16, k, m, rows16, present) == 0
+        assert np.array_equal(rows8, full) and np.array_equal(rows16, full)
+    assert (O.build_matrix(16, 200, 300)[200:] >> 8).any()  # points >= 256: tower coefficients
