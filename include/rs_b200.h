@@ -240,8 +240,9 @@ void rs_batch_free(rs_batch_t *batch);
  * still running. GF(2^8) requests admitted together share one launch group (one FFT
  * launch per (K,K) shape, one ragged matrix launch for the rest); GF(2^16) requests
  * with k + m <= 256 are validated as such and then run as GF(2^8) requests (their
- * coefficients lie in the subfield); other GF(2^16) requests run one per group; groups overlap on the server's streams. Results are the bytes
- * the single-stripe entry points produce. */
+ * coefficients lie in the subfield); other GF(2^16) requests run one per group;
+ * groups overlap on the server's streams. Results are the bytes the single-stripe
+ * entry points produce. */
 typedef struct {
   int field;                /* 8: ReedSolomon (k+m <= 256), 16: ReedSolomon16 (<= 65536) */
   int op;                   /* enum rs_batch_op */
