@@ -44,13 +44,31 @@ int log2_exact(uint64_t x) {
 
 // Table entry of a tower constant c (16 u16): the column bytes k_t * 2^p (p = 0..7) of
 // its Karatsuba factors k0 = c_lo, k1 = c_hi + c_lo, k2 = 32 c_hi, then 8 zero bytes.
+// Column words of GF(2^8) constants: for each a, the u16 pairs (a * 2^(2w)) |
+// (a * 2^(2w+1)) << 8 for w = 0..3, by repeated doubling modulo x^8+x^4+x^3+x^2+1.
+struct ColumnWords {
+  uint16_t w[256][4];
+  ColumnWords() {
+    for (int a = 0; a < 256; a++) {
+      uint8_t v = (uint8_t)a, b[8];
+      for (int q = 0; q < 8; q++) {
+        b[q] = v;
+        v = (uint8_t)((v << 1) ^ ((v & 0x80) ? 0x1d : 0));
+      }
+      for (int i = 0; i < 4; i++) w[a][i] = (uint16_t)(b[2 * i] | (b[2 * i + 1] << 8));
+    }
+  }
+};
+
 void push_const16(std::vector<uint16_t> &cols, uint16_t c) {
+  static const ColumnWords cw;
   const uint8_t hi = (uint8_t)(c >> 8), lo = (uint8_t)c;
   const uint8_t k[3] = {lo, (uint8_t)(hi ^ lo), gf8_mul(hi, 32)};
-  uint8_t bytes[32] = {};
+  const size_t at = cols.size();
+  cols.resize(at + 16);  // three factors' 4 words each, then 4 zero words
+  uint16_t *o = cols.data() + at;
   for (int t = 0; t < 3; t++)
-    for (int q = 0; q < 8; q++) bytes[t * 8 + q] = gf8_mul(k[t], (uint8_t)(1u << q));
-  for (int w = 0; w < 16; w++) cols.push_back((uint16_t)(bytes[2 * w] | (bytes[2 * w + 1] << 8)));
+    for (int i = 0; i < 4; i++) o[t * 4 + i] = cw.w[k[t]][i];
 }
 
 uint64_t push_const(Fft16Program &p, uint16_t c) {
@@ -59,12 +77,30 @@ uint64_t push_const(Fft16Program &p, uint16_t c) {
   return at;
 }
 
+// f(WHAT_l(beta ^ (j << (l + 1)))) for j = 0 .. count-1. WHAT_l is a normalised
+// subspace polynomial, which is GF(2)-linear, so consecutive values differ by the XOR of
+// its values on the low bits that flip from j-1 to j: one multiply chain per basis bit
+// instead of l multiplies per constant.
+template <class F>
+void for_level_consts(int l, uint32_t beta, uint32_t count, F &&f) {
+  const What16 &w = what16();
+  uint16_t flip[16];  // flip[t] = XOR of WHAT_l(2^(i + l + 1)) for i <= t
+  uint16_t acc = 0;
+  for (int i = 0; i < 16 && (1u << i) < count; i++) flip[i] = acc ^= w(l, (uint16_t)(1u << (i + l + 1)));
+  uint16_t v = w(l, (uint16_t)beta);
+  f(v);
+  for (uint32_t j = 1; j < count; j++) {
+    v ^= flip[__builtin_ctz(j)];
+    f(v);
+  }
+}
+
 // Constants of a transform of `size` registers at `beta`: (l, j) at size - (size >> l) + j.
 uint64_t push_transform(Fft16Program &p, uint32_t size, uint32_t beta) {
   uint64_t at = p.cols.size() / 16;
   const int lg = log2_exact(size);
-  for (int l = 0; l < lg; l++)
-    for (uint32_t j = 0; j < (size >> (l + 1)); j++) push_const(p, what16()(l, (uint16_t)(beta ^ (j << (l + 1)))));
+  p.cols.reserve(p.cols.size() + (size_t)16 * size);
+  for (int l = 0; l < lg; l++) for_level_consts(l, beta, size >> (l + 1), [&](uint16_t c) { push_const(p, c); });
   p.butterflies += (uint64_t)(size / 2) * lg;
   return at;
 }
@@ -184,9 +220,9 @@ bool fft16_decode_build(size_t k, size_t m, const std::vector<uint32_t> &survivo
   fwht(a);
   auto locator = [&](uint32_t x) { return T.exp[(a[x] / N) % 65535]; };
   auto push16 = [&](uint16_t c) { push_const16(d.cols, c); };
+  d.cols.reserve((size_t)16 * (2 * N + d.lg + targets.size()));
   // Transform constants (beta 0, both directions): (l, j) at N - (N >> l) + j.
-  for (uint32_t l = 0; l < d.lg; l++)
-    for (uint32_t j = 0; j < (N >> (l + 1)); j++) push16(what16()((int)l, (uint16_t)(j << (l + 1))));
+  for (uint32_t l = 0; l < d.lg; l++) for_level_consts((int)l, 0, N >> (l + 1), push16);
   // Row scales: L at the survivors, 0 elsewhere.
   d.row_off = d.cols.size() / 16;
   std::vector<uint16_t> scale(N, 0);
@@ -195,14 +231,14 @@ bool fft16_decode_build(size_t k, size_t m, const std::vector<uint32_t> &survivo
   // kappa_t = (product of the nonzero points of V_t) / W_t(2^t), since
   // W_t(x) = x * prod_{a in V_t, a != 0} (x - a).
   d.kappa_off = d.cols.size() / 16;
-  uint16_t prod = 1;
+  uint64_t log_prod = 0;  // in the log domain: prod = exp(log_prod)
   for (uint32_t t = 0; t < d.lg; t++) {
-    push16(gf16_mul(prod, what16().pivot_inv[t]));
-    for (uint32_t x = (1u << t); x < (2u << t); x++) prod = gf16_mul(prod, (uint16_t)x);
+    push16(gf16_mul(T.exp[log_prod % 65535], what16().pivot_inv[t]));
+    for (uint32_t x = (1u << t); x < (2u << t); x++) log_prod += T.log[x];
   }
-  // Target scales: 1 / L'(e).
+  // Target scales: 1 / L'(e) = exp(-log L'(e)).
   d.target_off = d.cols.size() / 16;
-  for (uint32_t e : targets) push16(gf16_inv(locator(e)));
+  for (uint32_t e : targets) push16(T.exp[(65535 - (a[e] / N) % 65535) % 65535]);
   d.butterflies = (uint64_t)3 * (N / 2) * d.lg + N + targets.size();
   return true;
 }
