@@ -339,8 +339,9 @@ class ReedSolomon16(_Coder):
         return out.reshape(self._m, self._k)
 
     def encode_route(self, shard_len=None, n_stripes=1):
-        """The shape's route, or with shard_len the route of an encode of n_stripes
-        stripes of that shard length."""
+        """The shape's route ("fft", "matrix", or "subfield" when k + m <= 256 and the
+        GF(2^8) codec of the shape does the work), or with shard_len the route of an
+        encode of n_stripes stripes of that shard length."""
         if shard_len is None:
             return self._L.rs16_encode_route(self._h).decode()
         return self._L.rs16_encode_route_for(self._h, shard_len, n_stripes).decode()
