@@ -99,7 +99,6 @@ void for_level_consts(int l, uint32_t beta, uint32_t count, F &&f) {
 uint64_t push_transform(Fft16Program &p, uint32_t size, uint32_t beta) {
   uint64_t at = p.cols.size() / 16;
   const int lg = log2_exact(size);
-  p.cols.reserve(p.cols.size() + (size_t)16 * size);
   for (int l = 0; l < lg; l++) for_level_consts(l, beta, size >> (l + 1), [&](uint16_t c) { push_const(p, c); });
   p.butterflies += (uint64_t)(size / 2) * lg;
   return at;
@@ -170,6 +169,9 @@ bool fft16_build(size_t k, size_t m, Fft16Program &p) {
   uint32_t t = 1;
   while (t < k) t <<= 1;
   p.t = t;
+  // Constants: interpolation transforms of t, t/2, ... registers (fewer than 2t), one
+  // per mulxor (at most log t) and t per evaluation coset (at most (k+m)/t + 1).
+  p.cols.reserve((size_t)16 * ((size_t)t * (3 + (k + m) / t) + 32));
   interpolate(p, 0, t, 0, (uint32_t)k);
   const uint64_t n = k + m;
   for (uint64_t beta = 0; beta < n; beta += t) {
@@ -184,6 +186,7 @@ bool fft16_build(size_t k, size_t m, Fft16Program &p) {
     p.evals.push_back(e);
   }
   p.eval_in_place = p.evals.size() == 1;
+  if (p.cols.capacity() > p.cols.size() + p.cols.size() / 2) p.cols.shrink_to_fit();
   return true;
 }
 
