@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "runtime.hpp"
+#include "codec8.hpp"
 #include "gf_host.hpp"
 #include "fft16.hpp"
 #include "kernels_fft.cuh"
@@ -148,7 +149,7 @@ static rs8_t *subfield(const rs16_codec *c) { return c->route.load() == 0 ? c->s
 static bool subfield_encode(const rs16_codec *c, size_t len, size_t n_stripes) {
   rs8_t *sub = subfield(c);
   if (!sub) return false;
-  if (std::strcmp(rs8_encode_route(sub, len), "matrix") != 0 || !c->gen->fft) return true;
+  if (use_fft8(sub, len) || !c->gen->fft) return true;
   return !fft16_faster_than_gf8_matrix(*c->gen->fft, len, std::max<size_t>(n_stripes, 1));
 }
 
