@@ -176,16 +176,25 @@ int rs8_reconstruct_batch_dev(rs8_t *codec, uint8_t *d_rows, size_t stripe_strid
  * process exits, and the host side stages through one fixed buffer: no cudaMalloc,
  * cudaFree or other allocating call is made. A call needing more than 8 MiB of working
  * memory (see rs8_reconstruct_batch_noalloc_limit) returns RS_ERR_TOO_LARGE; split the
- * batch. The first call on each device looks up the array's device address; make that
- * first call before capturing any stream on that device. Nothing in the array has to
- * start at zero: each call writes every entry it reads before reading it. Every call
- * shares the one array and it keeps the last call's contents: calls whose GPU work
- * overlaps (other streams, or other host threads) race on it, so run them one after
- * another. */
+ * batch. The first call on each device looks up the array's device address, which
+ * (with CUDA's default lazy module loading) loads this entry point's device code and
+ * reserves the 8 MiB array on that device then: make that first call at start-up,
+ * while memory is still free, and before capturing any stream on that device; it
+ * returns RS_ERR_CUDA if the device has no 8 MiB left. Later calls take no device
+ * memory. The index lists travel through a host buffer that the next call
+ * overwrites, so a call on a stream that is capturing returns RS_ERR_INVALID_ARGUMENT.
+ * Missing parity rows are rebuilt on the matrix route (one pass over the k
+ * survivors), never on the shape's compiled FFT or generator kernel: the bytes are the
+ * same as rs8_reconstruct_batch_dev's, the speed lower on shapes with such a kernel.
+ * Nothing in the array has to start at zero: each call writes every entry it reads
+ * before reading it. Every call shares the one array and it keeps the last call's
+ * contents: calls whose GPU work overlaps (other streams, or other host threads) race
+ * on it, so run them one after another. */
 int rs8_reconstruct_batch_noalloc(rs8_t *codec, uint8_t *d_rows, size_t stripe_stride,
                                   size_t n_stripes, size_t row_len, const uint8_t *present,
                                   int data_only, int *statuses, void *stream);
-/* Bytes of that fixed working area a call of this shape and stripe count needs. */
+/* Bytes of that fixed working area a call of this shape and stripe count needs
+ * (SIZE_MAX when the stripe count is beyond any working area). */
 size_t rs8_reconstruct_batch_noalloc_limit(size_t data_shards, size_t parity_shards,
                                            size_t n_stripes);
 

@@ -9,6 +9,7 @@
 // calls no cudaMalloc, cudaFree or allocating library routine.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 
 #include "codec8.hpp"
@@ -29,7 +30,11 @@ static std::mutex g_noalloc_mu;
 
 // Device address of g_noalloc_scratch per device. In host code the array's name is
 // only a host-side stand-in, so the address is looked up with cudaGetSymbolAddress,
-// once per device, with that device current (on the first call there).
+// once per device, with that device current (on the first call there). With CUDA's
+// lazy module loading that first lookup is also when this file's device module is
+// loaded, which is when the 8 MiB array is reserved on the device: the first call on
+// a device therefore does take device memory, once, and fails with RS_ERR_CUDA if the
+// device has no 8 MiB left. Later calls take none.
 constexpr int kMaxDevices = 64;
 static void *g_noalloc_dev_ptr[kMaxDevices];
 
@@ -50,6 +55,13 @@ static int noalloc_scratch(int device, uint8_t **out) {
 
 static size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Upper bound on the stripes one call can take: every stripe needs k*m + 2*(k+m) + 8
+// bytes of the working area, so any count above this is rejected before the layout's
+// products are formed (they could otherwise wrap around on 64-bit sizes).
+static size_t noalloc_max_stripes(size_t k, size_t m) {
+  return kNoAllocScratchBytes / (k * m + 2 * (k + m) + 8);
+}
+
 }  // namespace rsb
 
 using namespace rsb;
@@ -57,6 +69,9 @@ using namespace rsb;
 extern "C" {
 
 size_t rs8_reconstruct_batch_noalloc_limit(size_t k, size_t m, size_t n_stripes) {
+  // A stripe count that could not fit even one byte of working memory per entry is
+  // reported as "more than any size" instead of a product that wraps around.
+  if (n_stripes > noalloc_max_stripes(k, m)) return SIZE_MAX;
   return up256(n_stripes * k * 2) + up256(n_stripes * m * 2) + up256(n_stripes * 2) + up256(n_stripes * m * k) +
          up256(n_stripes * sizeof(int));
 }
@@ -69,16 +84,24 @@ int rs8_reconstruct_batch_noalloc(rs8_t *c, uint8_t *d_rows, size_t stripe_strid
   if (!d_rows) return RS_ERR_INVALID_ARGUMENT;
   const Gen8 &g = *c->gen;
   const size_t k = g.k, m = g.m, n = k + m;
+  if (n_stripes > noalloc_max_stripes(k, m)) return RS_ERR_TOO_LARGE;
   // Working-area layout: survivors | targets | target counts | decode rows | statuses.
   const size_t o_targ = up256(n_stripes * k * 2), o_nt = o_targ + up256(n_stripes * m * 2);
   const size_t o_rows = o_nt + up256(n_stripes * 2), o_stat = o_rows + up256(n_stripes * m * k);
   const size_t need = o_stat + up256(n_stripes * sizeof(int));
   if (need > kNoAllocScratchBytes) return RS_ERR_TOO_LARGE;
+  cudaStream_t st = (cudaStream_t)stream;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   RSB_CU(cudaSetDevice(g.device));
+  // The index lists are copied from g_noalloc_host, which the next call overwrites. A
+  // copy recorded into a graph would read that buffer only when the graph runs, by
+  // which time it may hold another call's lists, so a stream that is capturing is
+  // refused.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  RSB_CU(cudaStreamIsCapturing(st, &cap));
+  if (cap != cudaStreamCaptureStatusNone) return RS_ERR_INVALID_ARGUMENT;
   uint8_t *base = nullptr;
   RSB_TRY(noalloc_scratch(g.device, &base));
-  cudaStream_t st = (cudaStream_t)stream;
   uint16_t *surv = reinterpret_cast<uint16_t *>(g_noalloc_host);
   uint16_t *targ = reinterpret_cast<uint16_t *>(g_noalloc_host + o_targ);
   uint16_t *ntarg = reinterpret_cast<uint16_t *>(g_noalloc_host + o_nt);

@@ -2,7 +2,7 @@
 
 Run in a container that has the reference checkout (read-only) at REFERENCE_ROOT:
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT   (or REFERENCE_ROOT=... in the env)
 
 The reference is Rust and cannot be compiled here, so its golden data is read from
 its source text:
@@ -159,7 +159,9 @@ def gfni_golden(src):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT (or set REFERENCE_ROOT): the reference checkout")
     galois = read(root, "src/galois.rs")
     muls, exps = known_products(galois)
     g16 = read(root, "src/galois16.rs")

@@ -74,3 +74,49 @@ def test_noalloc_rejects_requests_beyond_its_working_area(gpu):
     present[:, 0] = 0
     code, _ = _noalloc(gpu, rs, rows, n_stripes, row_len, present)
     assert gpu.ERROR_NAMES[code] == "TooLarge"
+
+
+def test_noalloc_warm_calls_take_no_device_memory(gpu, O):
+    """After its first call on the device (which loads its device code and, with it,
+    the fixed working array), further calls leave the device's free memory as it was."""
+    import torch
+
+    k, m, row_len, n_stripes = 16, 16, 2048, 32
+    rs = gpu.ReedSolomon(k, m)
+    full, work, present = _stripes(O, k, m, row_len, n_stripes, seed=7)
+    rows = torch.from_numpy(work).cuda()
+    code, _ = _noalloc(gpu, rs, rows, n_stripes, row_len, present)  # warm-up
+    torch.cuda.synchronize()
+    assert code == 0
+    free_before = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        rows.copy_(torch.from_numpy(work))
+        code, _ = _noalloc(gpu, rs, rows, n_stripes, row_len, present)
+        assert code == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+    assert np.array_equal(rows.cpu().numpy(), full)
+
+
+def test_noalloc_refuses_a_capturing_stream(gpu, O):
+    """The index lists pass through a host buffer that the next call overwrites, so a
+    call made while its stream records a graph is refused instead of recorded."""
+    import torch
+
+    k, m, row_len, n_stripes = 10, 10, 512, 4
+    rs = gpu.ReedSolomon(k, m)
+    _, work, present = _stripes(O, k, m, row_len, n_stripes, seed=9)
+    rows = torch.from_numpy(work).cuda()
+    torch.cuda.synchronize()
+    L = gpu.load()
+    flags = np.ascontiguousarray(present, np.uint8)
+    side = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        graph.capture_begin()
+        code = L.rs8_reconstruct_batch_noalloc(
+            rs._h, rows.data_ptr(), (k + m) * row_len, n_stripes, row_len,
+            flags.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), 0, None, side.cuda_stream)
+        graph.capture_end()
+    assert gpu.ERROR_NAMES[code] == "InvalidArgument"
+    assert torch.equal(rows, torch.from_numpy(work).cuda())
