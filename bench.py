@@ -155,37 +155,83 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def cpu_baseline(seconds, threads=None):
-    """The oracle's multi-threaded GFNI replay of the reference FFT program, one stripe
-    per thread, looped over a bounded sample for about `seconds`."""
+def host_cpu():
+    """The host CPU as the baseline ran on it: model string, usable threads, ISA flags."""
+    model, flags = "unknown", set()
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name") and model == "unknown":
+                model = line.split(":", 1)[1].strip()
+            elif line.startswith("flags") and not flags:
+                flags = set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    usable = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    return {"model": model, "nproc": usable, "logical_cpus": os.cpu_count(),
+            "isa": [f for f in ("gfni", "avx512f", "avx512bw", "avx2") if f in flags]}
+
+
+def _check_cpu_parity(O, stripes, k, m):
+    """Byte-check the timed encoder's output against the oracle's scalar encode at
+    4096 sampled columns of the first and last stripe (encoding is column-wise)."""
+    rng = np.random.default_rng(11)
+    L = stripes.shape[2]
+    cols = np.sort(rng.choice(L, size=min(L, 4096), replace=False))
+    for s in (0, stripes.shape[0] - 1):
+        sub = np.ascontiguousarray(stripes[s][:, cols])
+        if not np.array_equal(sub[k:], O.encode8(k, m, sub[:k])):
+            raise RuntimeError("CPU baseline parity differs from the oracle (stripe %d)" % s)
+
+
+def cpu_baseline(seconds, threads=None, details=True):
+    """The oracle's restatement of the reference's x86 encode (straight-line GFNI/AVX-512
+    code generated from the LCH program, as the reference's macro-expanded zmm cores),
+    one stripe per thread on all usable host threads, looped over a bounded sample for
+    about `seconds`; byte-checked against the oracle after timing. Also one thread on
+    one cache-resident 10 KB stripe and one 1 MiB stripe, the sizes the reference
+    publishes for RS(32,32) (32,404 and 14,665 MiB/s payload on one Zen 5 core)."""
     from oracle import oracle as O
 
-    threads = threads or os.cpu_count()
+    k, m = K_DATA, M_PARITY
+    cpu = host_cpu()
+    threads = threads or cpu["nproc"]
     n_stripes = max(threads, 16)
     shard = SHARD
     rng = np.random.default_rng(7)
-    stripes = rng.integers(0, 256, size=(n_stripes, K_DATA + M_PARITY, shard), dtype=np.uint8)
+    stripes = rng.integers(0, 256, size=(n_stripes, k + m, shard), dtype=np.uint8)
     total_t, total_b, reps = 0.0, 0, 0
     while total_t < seconds:
-        total_t += O.encode8_batch_mt(K_DATA, M_PARITY, stripes, threads)
-        total_b += n_stripes * (K_DATA + M_PARITY) * shard
+        total_t += O.encode8_batch_mt(k, m, stripes, threads)
+        total_b += n_stripes * (k + m) * shard
         reps += 1
-    sample = ("%d stripes x RS(32,32) x 1 MiB shards, %d passes (%.1f s), %s path, one stripe per thread"
-              % (n_stripes, reps, total_t, "GFNI/AVX-512" if O.cpu_has_gfni() else "scalar"))
+    _check_cpu_parity(O, stripes, k, m)
+    single = {}
+    for label, L, budget in (("10KB", 10240, 1.0), ("1MiB", SHARD, 2.0)) if details else ():
+        one = rng.integers(0, 256, size=(k + m, L), dtype=np.uint8)
+        t1 = O.encode8_repeat(k, m, one, 1)
+        n = max(1, int(budget / max(t1, 1e-6)))
+        t = O.encode8_repeat(k, m, one, n)
+        single[label] = {"payload_mib_s": n * k * L / t / 2**20, "algorithmic_gbs": n * (k + m) * L / t / 1e9,
+                         "passes": n}
+    sample = ("%d stripes x RS(32,32) x 1 MiB shards, %d passes (%.1f s), one stripe per thread on %d threads, "
+              "%s path; byte-checked against the oracle" % (n_stripes, reps, total_t, threads,
+                                                            O.cpu_path(k, m, shard)))
     return {"value": total_b / total_t / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
-            "sample": sample}
+            "sample": sample, "cpu": cpu, "single_thread": single,
+            "published_single_thread_payload_mib_s": {"10KB": 32404, "1MiB": 14665,
+                                                      "host": "AMD Zen 5 (GCP c4d), 1 thread"}}
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
     steps = []
-    base = None
+    base = cpu_baseline(1.0)  # untimed: host details, single-thread rates, byte check
     for i in range(args.warmup + args.steps):
-        b = cpu_baseline(max(1.0, args.cpu_seconds / max(args.steps, 1)))
+        b = cpu_baseline(max(1.0, args.cpu_seconds / max(args.steps, 1)), details=False)
         if i >= args.warmup:
             steps.append(b["value"])
-        base = b
+            base["sample"] = b["sample"]
     value = statistics.mean(steps)
     # A step is our arm's step (args.stripes stripes of 1 MiB shards); the CPU time for it
     # is extrapolated from the bounded sample's rate.
@@ -198,7 +244,8 @@ def run_reference(args, rank):
                    "k": K_DATA, "m": M_PARITY, "shard_bytes": SHARD, "stripes_per_step": args.stripes},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "GB/s", "cores": base["cores"], "kind": "port",
-                         "sample": base["sample"]},
+                         "sample": base["sample"], "cpu": base["cpu"], "single_thread": base["single_thread"],
+                         "published_single_thread_payload_mib_s": base["published_single_thread_payload_mib_s"]},
         "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

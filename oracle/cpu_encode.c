@@ -2,11 +2,18 @@
  * CPU oracle: multi-threaded encode used as the timed CPU baseline.
  *
  * TEST INFRASTRUCTURE ONLY (see oracle.h). A C restatement of the reference's x86
- * encode fast path: the LCH flat program (src/fft.rs build_encode_program, the
- * generated lists of src/fft_programs.rs) replayed over 64-byte strips with one
- * GFNI affine multiply per program multiply (src/gf/fft_x86.rs:29-167,
- * src/gf/gfni.rs:12-64 for the 8x8 bit matrix of a constant), one stripe per
- * thread. Hosts without GFNI/AVX-512 fall back to the scalar table path.
+ * encode fast path, one stripe per thread:
+ *
+ * - the six generated shapes (7,13), (10,10), (14,14), (16,16), (18,6), (32,32) run
+ *   straight-line code with every program register in a zmm register and one
+ *   gf2p8affineqb per multiply, over 64-byte strips with an overlapped last strip,
+ *   as the reference's macro-expanded zmm cores do (src/macros.rs:1-45,
+ *   src/gf/fft_x86.rs:60-99, 149-211); that code is generated from the oracle's
+ *   LCH builder by gen_straight.c into _build/cpu_straight.c;
+ * - other shapes replay the same builder's flat program (src/fft.rs
+ *   build_encode_program) from memory, 4 strips per op;
+ * - shards shorter than one strip, or hosts without GFNI/AVX-512, take the scalar
+ *   table path.
  */
 #include <immintrin.h>
 #include <pthread.h>
@@ -32,8 +39,12 @@ static uint64_t gfni_matrix(uint8_t c) {
   return mat;
 }
 
+typedef void (*or_straight_fn)(const uint8_t *const *, uint8_t *const *, size_t);
+or_straight_fn or_straight_lookup(size_t k, size_t m); /* _build/cpu_straight.c */
+
 typedef struct {
   size_t k, m, len, n_stripes;
+  or_straight_fn straight;
   uint8_t *stripes;
   const lch_flat *prog;
   const uint64_t *mats; /* per op */
@@ -82,6 +93,10 @@ static void encode_stripe(job_t *jb, uint8_t *stripe, __m512i *regs) {
   uint8_t *out[256];
   for (size_t i = 0; i < k; i++) in[i] = stripe + i * len;
   for (size_t j = 0; j < m; j++) out[j] = stripe + (k + j) * len;
+  if (jb->straight && len >= 64) {
+    jb->straight(in, out, len);
+    return;
+  }
   const size_t block = 64 * STRIPS;
   size_t off = 0;
   if (jb->use_gfni && len >= block) {
@@ -128,6 +143,7 @@ double or_encode8_batch_mt(size_t k, size_t m, uint8_t *stripes, size_t n_stripe
   jb.mats = mats;
   __builtin_cpu_init();
   jb.use_gfni = __builtin_cpu_supports("gfni") && __builtin_cpu_supports("avx512bw");
+  jb.straight = jb.use_gfni ? or_straight_lookup(k, m) : NULL;
   pthread_mutex_init(&jb.lock, NULL);
   if (threads < 1) threads = 1;
   pthread_t *tid = (pthread_t *)malloc(threads * sizeof(pthread_t));
@@ -143,8 +159,46 @@ double or_encode8_batch_mt(size_t k, size_t m, uint8_t *stripes, size_t n_stripe
   return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
 }
 
+/* One thread encodes one stripe reps times after one untimed pass, as the
+ * reference's criterion benches time a stripe that stays in cache
+ * (benches/bench-harness/src/main.rs:100-117). Returns seconds for the reps. */
+double or_encode8_repeat(size_t k, size_t m, uint8_t *stripe, size_t len, size_t reps) {
+  lch_flat prog;
+  if (lch_build_flat(k, m, &prog)) return -1.0;
+  uint64_t *mats = (uint64_t *)malloc((prog.n_ops + 1) * sizeof(uint64_t));
+  for (size_t p = 0; p < prog.n_ops; p++) mats[p] = gfni_matrix(prog.ops[p].c);
+  job_t jb;
+  memset(&jb, 0, sizeof(jb));
+  jb.k = k;
+  jb.m = m;
+  jb.len = len;
+  jb.prog = &prog;
+  jb.mats = mats;
+  __builtin_cpu_init();
+  jb.use_gfni = __builtin_cpu_supports("gfni") && __builtin_cpu_supports("avx512bw");
+  jb.straight = jb.use_gfni ? or_straight_lookup(k, m) : NULL;
+  __m512i *regs = (__m512i *)aligned_alloc(64, (prog.register_count + 1) * STRIPS * 64);
+  encode_stripe(&jb, stripe, regs);
+  struct timespec t0, t1;
+  clock_gettime(CLOCK_MONOTONIC, &t0);
+  for (size_t r = 0; r < reps; r++) encode_stripe(&jb, stripe, regs);
+  clock_gettime(CLOCK_MONOTONIC, &t1);
+  free(regs);
+  free(mats);
+  lch_free_flat(&prog);
+  return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
+}
+
 /* Reports whether the GFNI path is used on this host (1) or the scalar one (0). */
 int or_cpu_has_gfni(void) {
   __builtin_cpu_init();
   return __builtin_cpu_supports("gfni") && __builtin_cpu_supports("avx512bw");
+}
+
+/* Path or_encode8_batch_mt takes for (k, m) at shard length len: 2 straight-line
+ * zmm code, 1 the program replayed from memory, 0 scalar. */
+int or_cpu_path(size_t k, size_t m, size_t len) {
+  if (!or_cpu_has_gfni()) return 0;
+  if (or_straight_lookup(k, m) && len >= 64) return 2;
+  return len >= 64 * STRIPS ? 1 : 0;
 }

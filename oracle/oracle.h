@@ -77,6 +77,14 @@ int or_reconstruct(int field, size_t k, size_t m, uint8_t *rows, const uint8_t *
 int or_decode_rows(int field, size_t k, size_t m, const uint8_t *present,
                    uint16_t *rows_out, size_t *n_rows);
 
+/* ---- column-sampled evaluation of the systematic code (eval_columns.c) ----
+ * data: k shards of len bytes back to back (split-plane wire for field 16). For each
+ * evaluation point x in points and each symbol column s in cols, out[p * n_cols + c] =
+ * f(x) where f (degree < k) has f(i) = data symbol i at column s: the shard at index x
+ * of the encoded stripe (src/reedsolomon.rs:155-159, src/field.rs:57-61). */
+int or_eval_columns(int field, size_t k, const uint8_t *data, size_t len, const uint32_t *cols,
+                    size_t n_cols, const uint32_t *points, size_t n_points, uint16_t *out);
+
 /* ---- LCH additive-FFT programs over GF(2^8), src/fft.rs ---- */
 /* Op encoding (one u32 per op): kind<<28 | dst<<18 | src<<8 | c, with
  * kind 0 = MulXor, 1 = Xor, 2 = MulCopy, 3 = Copy (src/fft.rs:87-97). */
@@ -96,8 +104,15 @@ void or_fft_what(uint8_t out[8 * 256]);
  * parity rows written. Returns elapsed seconds. */
 double or_encode8_batch_mt(size_t k, size_t m, uint8_t *stripes, size_t n_stripes,
                            size_t len, int threads);
+/* One thread, one stripe ((k+m) rows of len bytes) encoded reps times after an
+ * untimed pass (a cache-resident stripe, as the reference's benches time it).
+ * Returns seconds for the reps. */
+double or_encode8_repeat(size_t k, size_t m, uint8_t *stripe, size_t len, size_t reps);
 /* 1 when the GFNI/AVX-512 replay runs on this host, 0 for the scalar fallback. */
 int or_cpu_has_gfni(void);
+/* The path or_encode8_batch_mt takes: 2 straight-line zmm code (the six generated
+ * shapes, len >= 64), 1 program replay from memory, 0 scalar. */
+int or_cpu_path(size_t k, size_t m, size_t len);
 
 #ifdef __cplusplus
 }

@@ -59,6 +59,7 @@ def lib():
         L.or_fft_flat_run.argtypes = [_sz, _sz, _u8p, _u8p]
         L.or_fft_staged_run.argtypes = [_sz, _sz, _u8p, _u8p]
         L.or_fft_what.argtypes = [_u8p]
+        L.or_eval_columns.argtypes = [ctypes.c_int, _sz, _u8p, _sz, _u32p, _sz, _u32p, _sz, _u16p]
         L.or_encode8_batch_mt.restype = ctypes.c_double
         L.or_encode8_batch_mt.argtypes = [_sz, _sz, _u8p, _sz, _sz, ctypes.c_int]
         _lib = L
@@ -183,6 +184,33 @@ def decode_rows(field, k, m, present):
     return st, out[: n.value * k].reshape(n.value, k)
 
 
+def eval_columns(field, k, data, cols, points):
+    """Shard values of the encoded stripe at the given evaluation points (shard
+    indexes) and symbol columns, by barycentric Lagrange evaluation (O(k) per point and
+    column; eval_columns.c). data: (k, len) uint8, split-plane for field 16. Returns
+    (len(points), len(cols)) uint16 symbols."""
+    data = np.ascontiguousarray(data, dtype=np.uint8)
+    cols = np.ascontiguousarray(np.asarray(cols, dtype=np.uint32))
+    points = np.ascontiguousarray(np.asarray(points, dtype=np.uint32))
+    out = np.zeros((len(points), len(cols)), np.uint16)
+    st = lib().or_eval_columns(field, k, _p8(data), data.shape[1], cols.ctypes.data_as(_u32p), len(cols),
+                               points.ctypes.data_as(_u32p), len(points), _p16(out))
+    if st:
+        raise RuntimeError("eval_columns status %d" % st)
+    return out
+
+
+def symbols(field, shards, cols):
+    """The symbols of (rows, len) shards at the given symbol columns, as uint16:
+    GF(2^8) bytes, or tower symbols (high << 8) | low from the split-plane wire."""
+    shards = np.asarray(shards, dtype=np.uint8)
+    cols = np.asarray(cols, dtype=np.int64)
+    if field == 8:
+        return shards[:, cols].astype(np.uint16)
+    half = shards.shape[1] // 2
+    return (shards[:, half + cols].astype(np.uint16) << 8) | shards[:, cols]
+
+
 _KIND = {0: "mx", 1: "xo", 2: "mc", 3: "cp"}
 
 
@@ -252,5 +280,25 @@ def encode8_batch_mt(k, m, stripes, threads):
     return lib().or_encode8_batch_mt(k, m, _p8(stripes), stripes.shape[0], stripes.shape[2], threads)
 
 
+def encode8_repeat(k, m, stripe, reps):
+    """stripe: (k+m, len) uint8; one thread encodes it reps times (after one untimed
+    pass); returns seconds for the reps."""
+    assert stripe.flags["C_CONTIGUOUS"] and stripe.dtype == np.uint8
+    L = lib()
+    L.or_encode8_repeat.restype = ctypes.c_double
+    L.or_encode8_repeat.argtypes = [_sz, _sz, _u8p, _sz, _sz]
+    return L.or_encode8_repeat(k, m, _p8(stripe), stripe.shape[1], reps)
+
+
 def cpu_has_gfni():
     return bool(lib().or_cpu_has_gfni())
+
+
+_PATHS = {2: "straight-line GFNI/AVX-512 (generated)", 1: "GFNI/AVX-512 program replay", 0: "scalar"}
+
+
+def cpu_path(k, m, length):
+    """Which CPU encoder encode8_batch_mt runs for (k, m) at this shard length."""
+    L = lib()
+    L.or_cpu_path.argtypes = [_sz, _sz, _sz]
+    return _PATHS[L.or_cpu_path(k, m, length)]

@@ -54,9 +54,28 @@ def test_fft_route_1024x1024(gpu, O):
     rs.encode_batch_dev(d, p_mat, S, stripes)
     torch.cuda.synchronize()
     assert torch.equal(p_fft, p_mat)
+    # Both routes against the oracle at sampled symbol columns (both planes), every
+    # parity shard: the column evaluator is O(k) per point and column.
+    cols = _sample_cols(S // 2, 16, seed=11)
+    for s in range(stripes):
+        data = d[s].cpu().numpy()
+        want = O.eval_columns(16, k, data, cols, range(k, k + m))
+        assert np.array_equal(O.symbols(16, p_fft[s].cpu().numpy(), cols), want), s
 
 
-def test_fft_route_4096x12288_cosets(gpu):
+def _sample_cols(n_sym, count, seed):
+    """count symbol columns out of n_sym: both ends, the 32-symbol group edges next to
+    them, and random ones."""
+    rng = np.random.default_rng(seed)
+    fixed = [0, 31, 32, n_sym - 33, n_sym - 1]
+    rest = rng.choice(n_sym, size=count - len(fixed), replace=False)
+    return sorted(set(fixed) | set(int(c) for c in rest))
+
+
+def test_fft_route_4096x12288_cosets(gpu, O):
+    """(4096, 12288) at 2 KiB shards on the FFT route (many forward cosets) and on the
+    matrix route: equal to each other and, at 16 sampled symbol columns of both planes,
+    to the oracle's Lagrange evaluation for all 12288 parity shards."""
     import torch
 
     k, m, S = 4096, 12288, 2048
@@ -71,6 +90,10 @@ def test_fft_route_4096x12288_cosets(gpu):
     rs.set_route("matrix")
     rs.encode_batch_dev(d, p_mat, S, 1)
     torch.cuda.synchronize()
+    cols = _sample_cols(S // 2, 16, seed=12)
+    want = O.eval_columns(16, k, d[0].cpu().numpy(), cols, range(k, k + m))
+    assert np.array_equal(O.symbols(16, p_fft[0].cpu().numpy(), cols), want)
+    assert np.array_equal(O.symbols(16, p_mat[0].cpu().numpy(), cols), want)
     assert torch.equal(p_fft, p_mat)
 
 

@@ -143,10 +143,11 @@ def test_reconstruct_rows_and_options(gpu, O):
     assert all(np.array_equal(opt[i], full[i]) for i in range(k))
 
 
-def test_large_shape_round_trip(gpu):
-    """(4096, 12288) at 2 KiB shards: encode, erase m shards, rebuild, compare.
-    Too large for the symbol-wise oracle; decoding is unique, so the rebuilt stripe
-    must equal the original."""
+def test_large_shape_round_trip(gpu, O):
+    """(4096, 12288) at 2 KiB shards: encode, erase m shards, rebuild, compare. Too
+    large for the Gauss-Jordan oracle; decoding is unique, so the rebuilt stripe must
+    equal the original, and at 16 sampled symbol columns every shard (the rebuilt
+    ones included) must equal the oracle's Lagrange evaluation of the data."""
     import torch
 
     k, m, length = 4096, 12288, 2048
@@ -164,4 +165,8 @@ def test_large_shape_round_trip(gpu):
     full[torch.from_numpy(erased).cuda()] = 0
     rs.reconstruct_dev([full[i] for i in range(k + m)], present.tolist(), length)
     torch.cuda.synchronize()
+    rng_c = np.random.default_rng(45)
+    cols = sorted({0, 31, 32, length // 2 - 1} | set(int(c) for c in rng_c.choice(length // 2, 12, replace=False)))
+    want = O.eval_columns(16, k, data.cpu().numpy(), cols, range(k + m))
+    assert np.array_equal(O.symbols(16, full.cpu().numpy(), cols), want)
     assert torch.equal(full, ref)

@@ -176,3 +176,40 @@ def test_tower_subfield_shapes_equal_gf8_code(O):
         assert O.reconstruct(16, k, m, rows16, present) == 0
         assert np.array_equal(rows8, full) and np.array_equal(rows16, full)
     assert (O.build_matrix(16, 200, 300)[200:] >> 8).any()  # points >= 256: tower coefficients
+
+
+@pytest.mark.parametrize("field,k,m,length", [
+    (8, 1, 1, 5), (8, 10, 10, 100), (8, 32, 32, 64), (8, 7, 13, 33), (8, 128, 128, 40), (8, 3, 253, 9),
+    (16, 2, 1, 2), (16, 4, 2, 30), (16, 17, 33, 66), (16, 100, 200, 20), (16, 300, 20, 6)])
+def test_column_evaluator_matches_gauss_jordan_oracle(O, field, k, m, length):
+    """The barycentric column evaluator (used to check shapes too large for the O(k^3)
+    generator) gives every shard of the stripe the Gauss-Jordan oracle encodes."""
+    rng = np.random.default_rng(k * 1000 + m + field)
+    data = rng.integers(0, 256, size=(k, length), dtype=np.uint8)
+    parity = (O.encode8 if field == 8 else O.encode16)(k, m, data)
+    n_sym = length if field == 8 else length // 2
+    got = O.eval_columns(field, k, data, range(n_sym), range(k + m))
+    assert np.array_equal(got, O.symbols(field, np.concatenate([data, parity]), range(n_sym)))
+
+
+@pytest.mark.parametrize("k,m", [(7, 13), (10, 10), (14, 14), (16, 16), (18, 6), (32, 32), (20, 12), (4, 2)])
+def test_timed_cpu_encoder_matches_oracle(O, k, m):
+    """The multi-threaded CPU encoder timed as the baseline (straight-line GFNI code for
+    the six generated shapes, program replay or scalar otherwise) writes the oracle's
+    parity, for lengths below, at and between strips, with the overlapped last strip."""
+    rng = np.random.default_rng(k * 100 + m)
+    for length in (1, 31, 63, 64, 65, 127, 255, 256, 257, 1000, 4096 + 17):
+        stripes = rng.integers(0, 256, size=(3, k + m, length), dtype=np.uint8)
+        O.encode8_batch_mt(k, m, stripes, 2)
+        for s in range(3):
+            assert np.array_equal(stripes[s, k:], O.encode8(k, m, stripes[s, :k])), (length, s)
+        one = rng.integers(0, 256, size=(k + m, length), dtype=np.uint8)
+        O.encode8_repeat(k, m, one, 2)
+        assert np.array_equal(one[k:], O.encode8(k, m, one[:k])), length
+
+
+def test_timed_cpu_encoder_takes_straight_line_code_on_gfni_hosts(O):
+    if not O.cpu_has_gfni():
+        pytest.skip("host without GFNI/AVX-512: the scalar path is timed")
+    assert O.cpu_path(32, 32, 1 << 20).startswith("straight-line")
+    assert O.cpu_path(20, 12, 1 << 20) == "GFNI/AVX-512 program replay"
