@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--stripes", type=int, default=1024, help="stripes per step per GPU")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the untimed-region extras (reconstruct and mixed-batch figures)")
     ap.add_argument("--workload", default="encode",
                     choices=["encode", "stripes", "mixed", "rs16", "serve", "tuner"])
     ap.add_argument("--tuner-workloads", type=int, default=10000,
@@ -251,6 +253,18 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def device_parity_prefix(rs, shards, k, length):
+    """The first 64 parity bytes of row 0 recomputed by the device-resident batched encode
+    (a self-check of the host-pointer path, outside any timed region)."""
+    import torch
+
+    d = torch.from_numpy(np.stack([s[:64] for s in shards[:k]])).cuda()
+    p = torch.empty((1, rs.parity_shard_count(), 64), dtype=torch.uint8, device="cuda")
+    rs.encode_batch_dev(d[None], p, 64, 1)
+    torch.cuda.synchronize()
+    return p[0, 0].cpu().numpy()
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -340,6 +354,24 @@ def run_ours(args, rank, world):
     if not torch.equal(h_par[0].cuda(), parity[0]) or not torch.equal(h_par[S_e2e - 1].cuda(), parity[S_e2e - 1]):
         raise RuntimeError("end-to-end parity differs from the device-resident parity")
 
+    # The reference's own call shape: encode(&mut [T]) on one stripe of separately
+    # allocated (pageable) shards, copies and kernel inside the timed call.
+    single = {}
+    rng_h = np.random.default_rng(5)
+    for L1 in (65536, SHARD):
+        shards = [rng_h.integers(0, 256, size=L1, dtype=np.uint8) for _ in range(k)]
+        shards += [np.zeros(L1, np.uint8) for _ in range(m)]
+        rs.encode(shards)
+        reps = 40 if L1 == 65536 else 10
+        t_start = time.perf_counter()
+        for _ in range(reps):
+            rs.encode(shards)
+        t1s = (time.perf_counter() - t_start) / reps
+        if not np.array_equal(shards[k][:64], device_parity_prefix(rs, shards, k, L1)):
+            raise RuntimeError("single-stripe host encode differs from the device-resident encode")
+        single["%d" % L1] = {"gbs": (k + m) * L1 / t1s / 1e9, "payload_mib_s": k * L1 / t1s / 2**20,
+                             "ms_per_stripe": t1s * 1e3}
+
     hbm, hbm_kind = peaks()
     kern_avg = statistics.mean(kern_ms)
     achieved = bytes_per_step / (kern_avg * 1e-3) / 1e9
@@ -365,13 +397,38 @@ def run_ours(args, rank, world):
                          else "fallback 6.65 TB/s", "traffic_source": traffic_src},
             "e2e": {"value": e2e_gbs, "unit": "GB/s", "h2d_bytes_per_step": S_e2e * k * L,
                     "d2h_bytes_per_step": S_e2e * m * L,
-                    "path": "ReedSolomon.encode_batch_host (C ABI rs8_encode_batch) from pinned host memory"},
+                    "path": "ReedSolomon.encode_batch_host (C ABI rs8_encode_batch) from pinned host memory",
+                    "single_stripe_encode": dict(single, path="ReedSolomon.encode (C ABI rs8_encode), one stripe "
+                                                 "of separately allocated pageable shards per call")},
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
         if world == 1 and args.cpu_seconds > 0:  # 0 skips it (profiling runs)
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        if world == 1 and not args.no_extras:
+            del data, parity
+            torch.cuda.empty_cache()
+            line["also"] = extras()
         print(json.dumps(line), flush=True)
+
+
+def extras():
+    """Other configurations measured in the same run, after the headline (each GB/s is
+    algorithmic bytes over CUDA-event time; every reconstruct is checked bit-exact
+    against the pre-erasure stripes): RS(32,32) reconstruct of 1 MiB shards with 1..m
+    erasures per stripe, and the 10,000-stripe mixed batch (configuration 3) against one
+    plain call per stripe."""
+    from reed_solomon_b200 import workloads
+
+    rec = workloads.stripes_sweep(shapes=((32, 32),), sizes=(SHARD,), n_stripes=256, reps=3)[0]
+    mix = workloads.mixed_batch(n=10000, reps=3)
+    return {
+        "reconstruct_rs32x32_1MiB": {k2: rec[k2] for k2 in ("stripes", "reconstruct_gbs", "reconstruct_bit_exact",
+                                                             "encode_fft_gbs", "encode_matrix_gbs")},
+        "mixed_batch_10000": {k2: mix[k2] for k2 in ("stripes", "bytes", "batched_gbs", "batched_launches",
+                                                      "plain_gbs", "batched_over_plain", "create_s",
+                                                      "batched_matrix_only_gbs")},
+    }
 
 
 def run_workload(args):

@@ -522,6 +522,47 @@ int rs8_set_route(rs8_t *c, int route) {
   return RS_OK;
 }
 
+// Host shards of a stripe too large for one round trip to pay: the columns are cut into
+// chunks (encoding is column-wise, so each chunk is an independent stripe of shorter
+// shards) that rotate over the pipeline streams. Each chunk's shards are copied in, the
+// chunk is encoded, and its parity copied out on its stream; the copy-out of chunk c is
+// issued after chunk c + 1 is queued, because a copy into pageable host memory returns
+// only when it has finished: the next chunk's copy-in (another copy engine) and kernel
+// then run while it waits. Pinned shards make every copy asynchronous.
+static constexpr size_t kChunkStripeBytes = 8u << 20;  // data bytes per chunk (all shards)
+
+static int encode8_host_chunked(rs8_t *c, uint8_t *const *shards, size_t len) {
+  const Gen8 &g = *c->gen;
+  Exec &ex = *c->exec;
+  const size_t n = g.k + g.m;
+  const size_t cols = std::max<size_t>(4096, (kChunkStripeBytes / g.k) & ~size_t(4095));
+  const size_t n_chunks = (len + cols - 1) / cols;
+  RSB_TRY(ex.pipe_streams());
+  RSB_TRY(ex.pipe_buf.ensure(Exec::kPipe * n * cols));
+  auto copy_out = [&](size_t ch) -> int {
+    const size_t c0 = ch * cols, w = std::min(cols, len - c0);
+    const int slot = (int)(ch % Exec::kPipe);
+    uint8_t *base = ex.pipe_buf.ptr + slot * n * cols;
+    for (size_t j = 0; j < g.m; j++)
+      RSB_CU(cudaMemcpyAsync(shards[g.k + j] + c0, base + (g.k + j) * cols, w, cudaMemcpyDeviceToHost,
+                             ex.pipe[slot]));
+    return RS_OK;
+  };
+  for (size_t ch = 0; ch < n_chunks; ch++) {
+    const size_t c0 = ch * cols, w = std::min(cols, len - c0);
+    const int slot = (int)(ch % Exec::kPipe);
+    cudaStream_t st = ex.pipe[slot];
+    uint8_t *base = ex.pipe_buf.ptr + slot * n * cols;
+    for (size_t i = 0; i < g.k; i++)
+      RSB_CU(cudaMemcpyAsync(base + i * cols, shards[i] + c0, w, cudaMemcpyHostToDevice, st));
+    RSB_TRY(encode8_strided(c, base, cols, 0, base + g.k * cols, cols, 0, 1, w, st));
+    if (ch > 0) RSB_TRY(copy_out(ch - 1));
+  }
+  RSB_TRY(copy_out(n_chunks - 1));
+  for (auto st : ex.pipe) RSB_CU(cudaStreamSynchronize(st));
+  return RS_OK;
+}
+
 // src/reedsolomon.rs:271-278 then :701-722
 int rs8_encode(rs8_t *c, uint8_t *const *shards, size_t n_shards, size_t len) {
   if (!c || !shards) return RS_ERR_INVALID_ARGUMENT;
@@ -532,6 +573,7 @@ int rs8_encode(rs8_t *c, uint8_t *const *shards, size_t n_shards, size_t len) {
   Exec &ex = *c->exec;
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
+  if (g.k * len > 2 * kChunkStripeBytes) return encode8_host_chunked(c, shards, len);
   const size_t pitch = pitch16(len);
   RSB_TRY(ex.buf.ensure(n * pitch));
   for (size_t i = 0; i < g.k; i++)

@@ -1,0 +1,110 @@
+"""Host-memory entry points, the calls a real caller makes first (the reference's
+encode(&mut [T]) over separately allocated shards, src/reedsolomon.rs:271-351):
+
+* rs8_encode_batch, the pipelined many-stripe path, over more than its 64 MiB chunk
+  size, from pinned and from pageable memory, at a shard length that is not a multiple
+  of 16 (pitched device rows) and with stripes laid out data-then-parity (strided);
+* rs8_encode on one stripe large enough to be cut into column chunks that rotate over
+  the pipeline streams (with a ragged last chunk), from pageable and pinned shards.
+
+Parity is checked against the oracle's scalar encode at sampled columns (encoding is
+column-wise) and, on every byte, against the device-resident batched encode.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _cols(length, rng, count=2048):
+    """Sampled byte columns: both ends, 16-byte and chunk edges, and random ones."""
+    fixed = {0, 1, 15, 16, length - 1, length - 2}
+    for edge in (1 << 18, 2 << 18, 3 << 18, 4 << 18):
+        if edge < length:
+            fixed |= {edge - 1, edge}
+    rest = rng.choice(length, size=min(length, count), replace=False)
+    return np.array(sorted(fixed | set(int(c) for c in rest)))
+
+
+def _oracle_check(O, k, m, data, parity, rng):
+    """data: (k, len), parity: (m, len) of one stripe."""
+    cols = _cols(data.shape[1], rng)
+    d = np.ascontiguousarray(data[:, cols])
+    assert np.array_equal(parity[:, cols], O.encode8(k, m, d))
+
+
+def _device_parity(gpu, k, m, data):
+    """Every stripe's parity from the device-resident batched path: (S, m, len)."""
+    import torch
+
+    rs = gpu.ReedSolomon(k, m)
+    S, _, length = data.shape
+    d = torch.from_numpy(np.ascontiguousarray(data)).cuda()
+    p = torch.empty((S, m, length), dtype=torch.uint8, device="cuda")
+    rs.encode_batch_dev(d, p, length, S)
+    torch.cuda.synchronize()
+    return p.cpu().numpy()
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_host_batch_over_chunk_boundaries(gpu, O, pinned):
+    """RS(10,10), 11 stripes of 1 MiB + 5 bytes (about 110 MiB of data, so the 64 MiB
+    chunks split it three ways with a partial last chunk; rows pitched on the device)."""
+    import torch
+
+    k, m, length, S = 10, 10, (1 << 20) + 5, 11
+    rng = np.random.default_rng(31 + pinned)
+    if pinned:
+        data = torch.empty((S, k, length), dtype=torch.uint8, pin_memory=True).numpy()
+        parity = torch.zeros((S, m, length), dtype=torch.uint8, pin_memory=True).numpy()
+    else:
+        data = np.empty((S, k, length), np.uint8)
+        parity = np.zeros((S, m, length), np.uint8)
+    data[:] = rng.integers(0, 256, size=data.shape, dtype=np.uint8)
+    rs = gpu.ReedSolomon(k, m)
+    rs.encode_batch_host(data, parity, length, S)
+    assert np.array_equal(parity, _device_parity(gpu, k, m, data))
+    for s in (0, 5, S - 1):
+        _oracle_check(O, k, m, data[s], parity[s], rng)
+
+
+def test_host_batch_strided_stripes(gpu, O):
+    """Stripes stored whole (k data rows then m parity rows), 36 stripes of RS(32,32) x
+    64 KiB + 16 (144 MiB): data and parity strides of n rows."""
+    k, m, length, S = 32, 32, (64 << 10) + 16, 36
+    n = k + m
+    rng = np.random.default_rng(33)
+    stripes = rng.integers(0, 256, size=(S, n, length), dtype=np.uint8)
+    want = _device_parity(gpu, k, m, stripes[:, :k])
+    stripes[:, k:] = 0
+    rs = gpu.ReedSolomon(k, m)
+    flat = stripes.reshape(-1)
+    rs.encode_batch_host(flat, flat[k * length:], length, S, data_stride=n * length, parity_stride=n * length)
+    assert np.array_equal(stripes[:, k:], want)
+    _oracle_check(O, k, m, stripes[S - 1, :k], stripes[S - 1, k:], rng)
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_single_stripe_host_encode_in_column_chunks(gpu, O, pinned):
+    """One RS(32,32) stripe of 1 MiB + 333-byte shards, separately allocated (the
+    reference's Vec<u8> shards): 32 MiB of data, cut into column chunks on the device
+    with a ragged last chunk."""
+    import torch
+
+    k, m, length = 32, 32, (1 << 20) + 333
+    rng = np.random.default_rng(35 + pinned)
+    shards = []
+    for i in range(k + m):
+        if pinned:
+            a = torch.empty(length, dtype=torch.uint8, pin_memory=True).numpy()
+        else:
+            a = np.empty(length, np.uint8)
+        a[:] = rng.integers(0, 256, size=length, dtype=np.uint8) if i < k else 0xA5
+        shards.append(a)
+    rs = gpu.ReedSolomon(k, m)
+    rs.encode(shards)
+    data = np.stack(shards[:k])
+    parity = np.stack(shards[k:])
+    assert np.array_equal(parity, _device_parity(gpu, k, m, data[None])[0])
+    _oracle_check(O, k, m, data, parity, rng)
+    assert rs.verify(shards)
