@@ -369,6 +369,43 @@ int rs16_reconstruct_dev(rs16_t *codec, uint8_t *const *d_shards, const size_t *
                          const uint8_t *present, size_t n_shards, int data_only,
                          void *stream);
 
+/* ============================ payload framing ============================
+ * The steps the reference's callers take on either side of the coder, with no
+ * counterpart in the crate itself: shred-style FEC sets (the reference's Agave test
+ * shape, RS(32,32) x 987-byte shards, src/reedsolomon.rs:973) and the tape outer
+ * coder's segment chunking (benches/gf16-bench/src/bin/live.rs:1-16).
+ * A payload of payload_len bytes fills stripes of k data shards of shard_len bytes in
+ * order: byte p goes to stripe p / (k*shard_len), data shard (p / shard_len) % k,
+ * offset p % shard_len, and the rest of the last stripe's data shards is zero. Stripes
+ * are stored [stripe][k + m rows][shard_len] in device memory (d_stripes, n_stripes =
+ * rs_frame_stripe_count(...), else RS_INCORRECT_SHARD_SIZE; shard_len 0 ->
+ * RS_EMPTY_SHARD). */
+size_t rs_frame_stripe_count(size_t payload_len, size_t data_shards, size_t shard_len);
+/* Split d_payload into the stripes' data rows and encode every stripe's parity. */
+int rs8_frame_encode_dev(rs8_t *codec, const uint8_t *d_payload, size_t payload_len,
+                         size_t shard_len, uint8_t *d_stripes, size_t n_stripes, void *stream);
+/* Rebuild the missing data shards of every stripe (present: n_stripes x n host flags,
+ * the reference's data-only reconstruct) and reassemble the payload into d_payload.
+ * statuses (host, optional) gets each stripe's status; the return value is the first
+ * stripe's error (e.g. RS_TOO_FEW_SHARDS_PRESENT), whose payload bytes are then not
+ * rebuilt, or 0. */
+int rs8_frame_decode_dev(rs8_t *codec, uint8_t *d_stripes, size_t n_stripes, size_t shard_len,
+                         const uint8_t *present, uint8_t *d_payload, size_t payload_len,
+                         int *statuses, void *stream);
+/* The same over ReedSolomon16 (shard_len even; split-plane shards hold the payload's
+ * bytes in order). */
+int rs16_frame_encode_dev(rs16_t *codec, const uint8_t *d_payload, size_t payload_len,
+                          size_t shard_len, uint8_t *d_stripes, size_t n_stripes, void *stream);
+int rs16_frame_decode_dev(rs16_t *codec, uint8_t *d_stripes, size_t n_stripes, size_t shard_len,
+                          const uint8_t *present, uint8_t *d_payload, size_t payload_len,
+                          int *statuses, void *stream);
+/* Tape outer coder shape for a snapshot of `groups` groups: k = ceil(groups / 3) data
+ * shards, m = groups - k parity shards (errors as rs16_new's). */
+int rs_outer_shape(size_t groups, size_t *data_shards, size_t *parity_shards);
+/* Its shard size for a segment: ceil(segment_len / k) rounded up to a multiple of 64
+ * (at least 64); above 4 MiB -> RS_ERR_TOO_LARGE (the coder's "too much data"). */
+int rs_outer_shard_bytes(size_t segment_len, size_t data_shards, size_t *shard_bytes);
+
 /* ============================== gf slice kernels ============================== */
 
 /* gf::mul_slice / mul_slice_xor, src/gf/mod.rs:69-85: out[i] (^)= c * in[i] over

@@ -17,10 +17,13 @@ from .coder import (  # noqa: F401
     ReedSolomon16,
     RsError,
     device_check,
+    frame_stripe_count,
     kernel_launch_count,
     mul_slice,
     mul_slice_dev,
     mul_slice_xor,
+    outer_shape,
+    outer_shard_bytes,
 )
 from ._lib import LIB_PATH, load  # noqa: F401
 from .server import Server  # noqa: F401

@@ -94,6 +94,13 @@ SIGNATURES = {
     "rs16_encode_dev": (_int, [_vp, _pp, _sz, _sz, _vp]),
     "rs16_encode_batch_dev": (_int, [_vp, _vp, _sz, _vp, _sz, _sz, _sz, _vp]),
     "rs16_reconstruct_dev": (_int, [_vp, _pp, _szp, _u8p, _sz, _int, _vp]),
+    "rs_frame_stripe_count": (_sz, [_sz, _sz, _sz]),
+    "rs8_frame_encode_dev": (_int, [_vp, _vp, _sz, _sz, _vp, _sz, _vp]),
+    "rs8_frame_decode_dev": (_int, [_vp, _vp, _sz, _sz, _u8p, _vp, _sz, _intp, _vp]),
+    "rs16_frame_encode_dev": (_int, [_vp, _vp, _sz, _sz, _vp, _sz, _vp]),
+    "rs16_frame_decode_dev": (_int, [_vp, _vp, _sz, _sz, _u8p, _vp, _sz, _intp, _vp]),
+    "rs_outer_shape": (_int, [_sz, _szp, _szp]),
+    "rs_outer_shard_bytes": (_int, [_sz, _sz, _szp]),
     "rs_mlp_create": (_int, [_int, _int, _int, ctypes.c_uint64, _pp]),
     "rs_mlp_free": (None, [_vp]),
     "rs_mlp_param_count": (_sz, [_vp]),

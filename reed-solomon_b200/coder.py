@@ -258,6 +258,58 @@ class _Coder:
         _check(getattr(self._L, self._p + "_reconstruct_dev")(
             self._h, ptrs, lens, fp, len(shards), int(data_only), stream))
 
+    # ---- payload framing (rs*_frame_*: the callers' steps either side of the coder) ----
+    def frame_encode_dev(self, payload, shard_len, stream=0):
+        """payload: 1-D uint8 CUDA tensor -> stripes (S, n, shard_len) on the device: the
+        payload's bytes fill the data shards in order (zeros after it), parity encoded."""
+        import torch
+
+        length = payload.numel()
+        S = frame_stripe_count(length, self._k, shard_len)
+        stripes = torch.empty((S, self._k + self._m, shard_len), dtype=torch.uint8, device=payload.device)
+        _check(getattr(self._L, self._p + "_frame_encode_dev")(
+            self._h, _dev_ptr(payload) if length else None, length, shard_len,
+            _dev_ptr(stripes) if S else None, S, stream))
+        return stripes
+
+    def frame_decode_dev(self, stripes, shard_len, present, payload_len, stream=0):
+        """Rebuild every stripe's missing data shards (present: (S, n) flags) and
+        reassemble the payload. Returns (payload tensor, per-stripe statuses): a stripe
+        with too few shards reports its error there (its payload bytes are not rebuilt);
+        argument and device errors raise."""
+        import torch
+
+        S = stripes.shape[0] if stripes.dim() else 0
+        f = np.ascontiguousarray(np.asarray(present, dtype=np.uint8).reshape(S, self._k + self._m))
+        out = torch.empty(payload_len, dtype=torch.uint8, device=stripes.device)
+        st = (ctypes.c_int * max(S, 1))()
+        code = getattr(self._L, self._p + "_frame_decode_dev")(
+            self._h, _dev_ptr(stripes) if S else None, S, shard_len,
+            f.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), _dev_ptr(out) if payload_len else None,
+            payload_len, st, stream)
+        if code >= 100 or code in (9, 11):
+            _check(code)
+        return out, list(st)[:S]
+
+
+def frame_stripe_count(payload_len, data_shards, shard_len):
+    """Stripes a payload fills at k data shards of shard_len bytes each."""
+    return _lib.load().rs_frame_stripe_count(payload_len, data_shards, shard_len)
+
+
+def outer_shape(groups):
+    """The tape outer coder's (k, m) for `groups` groups: k = ceil(groups / 3)."""
+    k, m = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    _check(_lib.load().rs_outer_shape(groups, ctypes.byref(k), ctypes.byref(m)))
+    return k.value, m.value
+
+
+def outer_shard_bytes(segment_len, data_shards):
+    """The outer coder's shard size: ceil(segment / k) rounded up to 64, at most 4 MiB."""
+    s = ctypes.c_size_t(0)
+    _check(_lib.load().rs_outer_shard_bytes(segment_len, data_shards, ctypes.byref(s)))
+    return s.value
+
 
 class ReedSolomon(_Coder):
     """ReedSolomon over GF(2^8), src/reedsolomon.rs:139-196."""
