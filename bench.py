@@ -54,6 +54,8 @@ def parse():
                     help="skip the untimed-region extras (reconstruct and mixed-batch figures)")
     ap.add_argument("--workload", default="encode",
                     choices=["encode", "stripes", "mixed", "rs16", "serve", "tuner"])
+    ap.add_argument("--save-model", default=None,
+                    help="tuner workload: write the trained cost model here and its timings beside it (.npz)")
     ap.add_argument("--tuner-workloads", type=int, default=10000,
                     help="workloads the tuner times (about 5 applicable configurations each)")
     ap.add_argument("--requests", type=int, default=400, help="requests of the serve workload")
@@ -427,7 +429,8 @@ def extras():
                                                              "encode_fft_gbs", "encode_matrix_gbs")},
         "mixed_batch_10000": {k2: mix[k2] for k2 in ("stripes", "bytes", "batched_gbs", "batched_launches",
                                                       "plain_gbs", "batched_over_plain", "create_s",
-                                                      "batched_matrix_only_gbs")},
+                                                      "batched_matrix_only_gbs", "model_gbs", "exhaustive_gbs",
+                                                      "regret_model", "regret_default") if k2 in mix},
     }
 
 
@@ -465,7 +468,9 @@ def run_workload(args):
                 res = workloads.rs16_shapes()
             line = {"metric": "ReedSolomon16 encode/reconstruct GB/s", "unit": "GB/s", "results": res}
         elif args.workload == "tuner":
-            res = workloads.tuner_regret(n_workloads=args.tuner_workloads)
+            save_t = os.path.splitext(args.save_model)[0] + "_timings.npz" if args.save_model else None
+            res = workloads.tuner_regret(n_workloads=args.tuner_workloads, save_model=args.save_model,
+                                         save_timings=save_t)
             line = {"metric": "cost-model route/tile regret vs exhaustive tuning (held out)", "unit": "fraction",
                     "value": res["regret_model"], "higher_is_better": False, "results": res}
         else:

@@ -227,6 +227,35 @@ typedef struct {
 typedef struct rs_batch rs_batch_t;
 int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *statuses,
                     rs_batch_t **out);
+/* rs_batch_create with a launch configuration per encode item (configs[i], an index
+ * into the tuner's configurations, rs_tuning_config; -1 = the library's automatic
+ * choice): matrix configurations put the item on the ragged matrix launch, FFT and
+ * generator configurations on the shape's compiled kernel with that launch shape (one
+ * launch per shape and configuration); a configuration the item's shape has no kernel
+ * for gives the item RS_ERR_INVALID_ARGUMENT. Reconstruct items ignore it. Results are
+ * the same bytes whatever the configurations. */
+int rs_batch_create_configured(const rs_batch_item *items, size_t n_items, int flags,
+                               const int *configs, int *statuses, rs_batch_t **out);
+typedef struct rs_mlp rs_mlp_t;
+/* The cost model's choice for a batch: encode items of shapes with a compiled kernel
+ * are grouped by shape and row alignment (each group is one launch); the model (an
+ * rs_mlp_t with rs_tuning_features inputs and rs_tuning_config_count outputs, e.g. one
+ * loaded with rs_mlp_load) predicts every item's log time per configuration from
+ * (k, m, row bytes, erasures 0, stripes in its group, alignment), and each group gets
+ * the applicable configuration with the least predicted total where that is predicted
+ * at least 10% faster than the library's automatic choice (else -1, the automatic
+ * choice). configs[i] = -1 for every other item. Pass the result to
+ * rs_batch_create_configured. */
+int rs_batch_choose(const rs_batch_item *items, size_t n_items, rs_mlp_t *model, int *configs);
+/* Launch configurations the autotuner times and the cost model scores: index 0..count-1
+ * -> route (0 matrix, 1 FFT, 2 generator kernel), p0 (matrix tile variant, or FFT
+ * lane-group width 0 narrow / 1 wide), p1 (FFT launch shape, rs_set_fft_variant). */
+int rs_tuning_config_count(void);
+int rs_tuning_config(int index, int *route, int *p0, int *p1);
+/* Inputs of the cost model: log2(k)/8, log2(m)/8, log2(row bytes)/20, erasures/m,
+ * log2(stripes per launch)/8 (a launch group is scored as at most 512 stripes and at
+ * most 64 MiB, the autotuner's range), 1 when rows are not 16-byte aligned. */
+int rs_tuning_features(void);
 /* Enqueues one replay of the batch on `stream`. */
 int rs_batch_launch(rs_batch_t *batch, void *stream);
 /* Kernel launches per replay, stripes on each route (a stripe with any matrix work
@@ -278,6 +307,9 @@ typedef struct {
   int streams;              /* device streams (0: 4) */
   int max_batch;            /* GF(2^8) requests per launch group (0: 64) */
   int lookahead;            /* queued requests that may pass a head that does not fit */
+  struct rs_mlp *model;     /* cost model choosing each FFT launch group's launch shape
+                               (rs_batch_choose's inputs and outputs; null: the library's
+                               automatic choice); must outlive the server */
 } rs_server_config;
 typedef struct {
   uint64_t submitted, completed, rejected;
@@ -420,8 +452,13 @@ int gf8_mul_slice_dev(uint8_t *d_out, const uint8_t *d_in, size_t n, uint8_t c, 
  * trained and evaluated on the GPU by this library's kernels; the tuner maps a
  * workload's features to one predicted log-time per candidate launch configuration.
  * Device arrays are row-major float: x [batch x n_in], y and mask [batch x n_out]. */
-typedef struct rs_mlp rs_mlp_t;
 int rs_mlp_create(int n_in, int hidden, int n_out, uint64_t seed, rs_mlp_t **out);
+/* Input, hidden and output widths. */
+int rs_mlp_dims(const rs_mlp_t *mlp, int *n_in, int *hidden, int *n_out);
+/* The network to a file and back (magic, widths, float32 parameters). A file that is
+ * not such a network -> RS_ERR_INVALID_ARGUMENT. */
+int rs_mlp_save(const rs_mlp_t *mlp, const char *path);
+int rs_mlp_load(const char *path, rs_mlp_t **out);
 void rs_mlp_free(rs_mlp_t *mlp);
 size_t rs_mlp_param_count(const rs_mlp_t *mlp);
 int rs_mlp_get_params(const rs_mlp_t *mlp, float *out, size_t n);

@@ -62,6 +62,11 @@ SIGNATURES = {
     "rs8_reconstruct_batch_noalloc": (_int, [_vp, _vp, _sz, _sz, _sz, _u8p, _int, _intp, _vp]),
     "rs8_reconstruct_batch_noalloc_limit": (_sz, [_sz, _sz, _sz]),
     "rs_batch_create": (_int, [_vp, _sz, _int, _intp, _pp]),
+    "rs_batch_create_configured": (_int, [_vp, _sz, _int, _intp, _intp, _pp]),
+    "rs_batch_choose": (_int, [_vp, _sz, _vp, _intp]),
+    "rs_tuning_config_count": (_int, []),
+    "rs_tuning_config": (_int, [_int, _intp, _intp, _intp]),
+    "rs_tuning_features": (_int, []),
     "rs_batch_launch": (_int, [_vp, _vp]),
     "rs_batch_stats": (_int, [_vp, _szp, _szp, _szp, ctypes.POINTER(ctypes.c_uint64)]),
     "rs_batch_free": (None, [_vp]),
@@ -103,6 +108,9 @@ SIGNATURES = {
     "rs_outer_shard_bytes": (_int, [_sz, _sz, _szp]),
     "rs_mlp_create": (_int, [_int, _int, _int, ctypes.c_uint64, _pp]),
     "rs_mlp_free": (None, [_vp]),
+    "rs_mlp_dims": (_int, [_vp, _intp, _intp, _intp]),
+    "rs_mlp_save": (_int, [_vp, ctypes.c_char_p]),
+    "rs_mlp_load": (_int, [ctypes.c_char_p, _pp]),
     "rs_mlp_param_count": (_sz, [_vp]),
     "rs_mlp_get_params": (_int, [_vp, _vp, _sz]),
     "rs_mlp_set_params": (_int, [_vp, _vp, _sz]),

@@ -482,9 +482,14 @@ MATRIX_ONLY, NO_GRAPH = 1, 2
 class Batch:
     """A mixed batch of GF(2^8) stripes (rs_batch_create): items are tuples
     (codec, rows, row_stride, row_len, op, present) with `rows` a CUDA tensor or device
-    pointer holding n = k+m rows; `present` (n flags) for reconstruct ops."""
+    pointer holding n = k+m rows; `present` (n flags) for reconstruct ops.
 
-    def __init__(self, items, flags=0):
+    Launch configurations: `configs` gives one per item (an index into
+    tuner.CONFIGS, -1 automatic; rs_batch_create_configured); `model` (a
+    tuner.CostModel, e.g. tuner.shipped_model()) lets the cost model choose them
+    (rs_batch_choose). Neither changes the bytes."""
+
+    def __init__(self, items, flags=0, configs=None, model=None):
         self._L = _lib.load()
         n = len(items)
         arr = (_BatchItem * max(n, 1))()
@@ -502,7 +507,16 @@ class Batch:
         self._codecs = [it[0] for it in items]
         st = (ctypes.c_int * max(n, 1))()
         h = ctypes.c_void_p()
-        _check(self._L.rs_batch_create(arr, n, flags, st, ctypes.byref(h)))
+        if model is not None:
+            cfg = (ctypes.c_int * max(n, 1))()
+            _check(self._L.rs_batch_choose(arr, n, model._h, cfg))
+            configs = list(cfg)[:n]
+        self.configs = list(configs) if configs is not None else None
+        if configs is None:
+            _check(self._L.rs_batch_create(arr, n, flags, st, ctypes.byref(h)))
+        else:
+            cfg = (ctypes.c_int * max(n, 1))(*configs)
+            _check(self._L.rs_batch_create_configured(arr, n, flags, cfg, st, ctypes.byref(h)))
         self._h = h
         self.statuses = list(st)[:n]
 

@@ -31,6 +31,7 @@
 #include <utility>
 
 #include "kernels_matrix.cuh"
+#include "tuning.hpp"
 
 namespace rsb {
 
@@ -442,6 +443,10 @@ struct FftArgs {
   int use_store_bits;
   // Ragged form: some item's rows are not 16-byte aligned (chooses the launch shape).
   int items_unaligned;
+  // Launch configuration of this launch (the cost model's or a caller's choice), -1 for
+  // the shape's current setting: lane-group width (0 narrow, 1 wide) and launch shape
+  // (index into kFftVariants).
+  int cfg_wide = -1, cfg_variant = -1;
 };
 
 __device__ __forceinline__ bool fft_store_row(const FftArgs &a, uint32_t unit, uint32_t row) {
@@ -889,6 +894,22 @@ inline int &fft_lanes_choice(int K) {
   return c[l & 7];
 }
 
+// The tuner-table entry (tuning.hpp) of the library's automatic choice for a launch of
+// this compiled shape: its generator kernel, or the (K,K) shape's current FFT launch
+// shape, or on unaligned rows the wide-lane shape of its unaligned kernel; -1 when no
+// entry matches.
+inline int fft_auto_config(const FftShape &sh, bool aligned) {
+  if (sh.gen) return kTuneConfigCount - 1;
+  int wide = fft_lanes_choice(sh.k), variant = fft_variant_for(sh.k);
+  if (!aligned && sh.k >= 16 && fft_shape_auto(sh.k)) {
+    wide = 1;
+    variant = fft_unaligned_variant(sh.k);
+  }
+  for (int c = 0; c < kTuneConfigCount; c++)
+    if (kTuneConfigs[c].route == kTuneFft && kTuneConfigs[c].p0 == wide && kTuneConfigs[c].p1 == variant) return c;
+  return -1;
+}
+
 template <int K, int W, bool PTRS, int V, bool UNAL = false>
 inline cudaError_t launch_fft_kwv(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
   constexpr FftVariant var = kFftVariants[V];
@@ -919,14 +940,16 @@ inline cudaError_t launch_fft_kw(const FftArgs &a, const PtrTableT<PTRS> &pt, cu
 
 template <int K, bool PTRS>
 inline cudaError_t launch_fft_k(const FftArgs &a, const PtrTableT<PTRS> &pt, cudaStream_t st) {
-  const int wide = fft_lanes_choice(K), variant = fft_variant_for(K);
+  const bool forced = a.cfg_variant >= 0 || a.cfg_wide >= 0;
+  const int wide = a.cfg_wide >= 0 ? a.cfg_wide : fft_lanes_choice(K);
+  const int variant = a.cfg_variant >= 0 ? a.cfg_variant : fft_variant_for(K);
   if constexpr (!PTRS && K >= 16) {
     const bool unaligned =
         a.items ? a.items_unaligned != 0
                 : ((reinterpret_cast<uintptr_t>(a.in_base) | reinterpret_cast<uintptr_t>(a.out_base) |
                     a.in_row_stride | a.in_stripe_stride | a.out_row_stride | a.out_stripe_stride) &
                    15u) != 0;
-    if (unaligned && fft_shape_auto(K))
+    if (unaligned && fft_shape_auto(K) && !forced)
       return launch_fft_kwv<K, fft_w_hi(K), PTRS, fft_unaligned_variant(K), true>(a, pt, st);
   }
   if constexpr (fft_w_lo(K) == fft_w_hi(K)) {
@@ -1033,13 +1056,15 @@ inline int launch_fft8(const FftShape &sh, const uint8_t *in_base, uint64_t in_r
 // Ragged batch of (K, K) stripes described by a device item array.
 inline int launch_fft8_items(const FftShape &sh, const FftItem *d_items, uint32_t n_items,
                              uint64_t total_groups, cudaStream_t st, const uint32_t *store_mask = nullptr,
-                             bool items_unaligned = false) {
+                             bool items_unaligned = false, int cfg_wide = -1, int cfg_variant = -1) {
   FftArgs a{};
   a.items = d_items;
   a.n_items = n_items;
   a.total_groups = total_groups;
   a.store_mask = store_mask;
   a.items_unaligned = items_unaligned;
+  a.cfg_wide = cfg_wide;
+  a.cfg_variant = cfg_variant;
   PtrTableT<false> pt{};
   return launch_fft_any<false>(sh, a, pt, st);
 }

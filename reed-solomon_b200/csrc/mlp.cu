@@ -9,7 +9,9 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <random>
 #include <vector>
@@ -115,6 +117,7 @@ static __global__ void mlp_adam(float *p, const float *g, float *m1, float *m2, 
 using namespace rsb;
 
 struct rs_mlp {
+  std::mutex mu;  // predict and training share the work buffers
   int device = 0;
   MlpShape shape;
   float *params = nullptr, *grads = nullptr, *m1 = nullptr, *m2 = nullptr;
@@ -259,8 +262,63 @@ int rs_mlp_set_params(rs_mlp_t *m, const float *in, size_t n) {
   return RS_OK;
 }
 
+int rs_mlp_dims(const rs_mlp_t *m, int *n_in, int *hidden, int *n_out) {
+  if (!m) return RS_ERR_INVALID_ARGUMENT;
+  if (n_in) *n_in = m->shape.dims[0];
+  if (hidden) *hidden = m->shape.dims[1];
+  if (n_out) *n_out = m->shape.dims[kMlpLayers];
+  return RS_OK;
+}
+
+// File: 8-byte magic "RSMLP\0\0\1", then int32 n_in, hidden, n_out, then the parameters
+// as little-endian float32 in parameter order.
+static const char kMlpMagic[8] = {'R', 'S', 'M', 'L', 'P', 0, 0, 1};
+
+int rs_mlp_save(const rs_mlp_t *m, const char *path) {
+  if (!m || !path) return RS_ERR_INVALID_ARGUMENT;
+  std::vector<float> p(m->shape.total);
+  RSB_TRY(rs_mlp_get_params(m, p.data(), p.size()));
+  FILE *f = fopen(path, "wb");
+  if (!f) return RS_ERR_INVALID_ARGUMENT;
+  const int32_t dims[3] = {m->shape.dims[0], m->shape.dims[1], m->shape.dims[kMlpLayers]};
+  bool ok = fwrite(kMlpMagic, 1, 8, f) == 8 && fwrite(dims, 4, 3, f) == 3 &&
+            fwrite(p.data(), 4, p.size(), f) == p.size();
+  ok = (fclose(f) == 0) && ok;
+  return ok ? RS_OK : RS_ERR_INVALID_ARGUMENT;
+}
+
+int rs_mlp_load(const char *path, rs_mlp_t **out) {
+  if (!path || !out) return RS_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  FILE *f = fopen(path, "rb");
+  if (!f) return RS_ERR_INVALID_ARGUMENT;
+  char magic[8];
+  int32_t dims[3];
+  if (fread(magic, 1, 8, f) != 8 || memcmp(magic, kMlpMagic, 8) != 0 || fread(dims, 4, 3, f) != 3 ||
+      dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0 || dims[0] > 4096 || dims[1] > 4096 || dims[2] > 4096) {
+    fclose(f);
+    return RS_ERR_INVALID_ARGUMENT;
+  }
+  rs_mlp_t *m = nullptr;
+  int st = rs_mlp_create(dims[0], dims[1], dims[2], 0, &m);
+  if (st) {
+    fclose(f);
+    return st;
+  }
+  std::vector<float> p(m->shape.total);
+  const bool ok = fread(p.data(), 4, p.size(), f) == p.size();
+  fclose(f);
+  if (!ok || (st = rs_mlp_set_params(m, p.data(), p.size())) != RS_OK) {
+    delete m;
+    return ok ? st : RS_ERR_INVALID_ARGUMENT;
+  }
+  *out = m;
+  return RS_OK;
+}
+
 int rs_mlp_predict(rs_mlp_t *m, const float *d_x, int batch, float *d_out) {
   if (!m || !d_x || !d_out || batch <= 0) return RS_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(m->mu);
   RSB_CU(cudaSetDevice(m->device));
   RSB_TRY(mlp_forward(m, d_x, batch));
   RSB_CU(cudaMemcpyAsync(d_out, m->act(kMlpLayers, batch), sizeof(float) * batch * m->shape.dims[kMlpLayers],
@@ -272,6 +330,7 @@ int rs_mlp_predict(rs_mlp_t *m, const float *d_x, int batch, float *d_out) {
 int rs_mlp_gradients(rs_mlp_t *m, const float *d_x, const float *d_y, const float *d_mask, int batch,
                      float mask_count, float *grads_out, size_t n, float *loss) {
   if (!m || !d_x || !d_y || !d_mask || batch <= 0) return RS_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(m->mu);
   RSB_CU(cudaSetDevice(m->device));
   RSB_TRY(mlp_forward(m, d_x, batch));
   RSB_TRY(mlp_backward(m, d_y, d_mask, batch, mask_count));
@@ -289,6 +348,7 @@ int rs_mlp_gradients(rs_mlp_t *m, const float *d_x, const float *d_y, const floa
 int rs_mlp_train_step(rs_mlp_t *m, const float *d_x, const float *d_y, const float *d_mask, int batch,
                       float mask_count, float lr, float *loss) {
   if (!m || !d_x || !d_y || !d_mask || batch <= 0) return RS_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(m->mu);
   RSB_CU(cudaSetDevice(m->device));
   RSB_TRY(mlp_forward(m, d_x, batch));
   RSB_TRY(mlp_backward(m, d_y, d_mask, batch, mask_count));

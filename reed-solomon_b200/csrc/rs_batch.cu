@@ -19,6 +19,7 @@
 #include "kernels_fft.cuh"
 #include "kernels_plan.cuh"
 #include "runtime.hpp"
+#include "tuning.hpp"
 
 using namespace rsb;
 
@@ -37,6 +38,7 @@ struct rs_batch {
     uint64_t groups;
     const uint32_t *masks;  // parity rows to store per item; null: every row
     bool unaligned;         // some item's rows are not 16-byte aligned
+    int cfg_wide = -1, cfg_variant = -1;  // FFT launch configuration (-1: the shape's)
   };
   std::vector<FftLaunch> ffts;    // encodes
   std::vector<FftLaunch> regens;  // missing parity of reconstructs, after the data rows
@@ -57,7 +59,8 @@ struct rs_batch {
 namespace rsb {
 
 static int batch_enqueue(rs_batch *b, cudaStream_t st) {
-  for (const auto &f : b->ffts) RSB_TRY(launch_fft8_items(*f.shape, f.items, f.n, f.groups, st, nullptr, f.unaligned));
+  for (const auto &f : b->ffts)
+    RSB_TRY(launch_fft8_items(*f.shape, f.items, f.n, f.groups, st, nullptr, f.unaligned, f.cfg_wide, f.cfg_variant));
   if (b->n_ragged) {
     gf8_ragged_kernel<8><<<(unsigned)b->ragged_blocks, kThreads, b->ragged_smem, st>>>(b->ragged, b->n_ragged);
     g_launches++;
@@ -84,11 +87,129 @@ struct Arena {
   }
 };
 
+// A compiled-kernel launch group: the shape and, for FFT shapes, a launch configuration.
+struct FftKey {
+  const FftShape *shape;
+  int wide, variant;
+  bool operator<(const FftKey &o) const {
+    if (shape != o.shape) return shape < o.shape;
+    if (wide != o.wide) return wide < o.wide;
+    return variant < o.variant;
+  }
+};
+
+static bool rows_aligned(const rs_batch_item &it) {
+  return ((reinterpret_cast<uintptr_t>(it.d_rows) | it.row_stride) & 15u) == 0;
+}
+
+static int batch_create(const rs_batch_item *items, size_t n_items, int flags, const int *configs, int *statuses,
+                        rs_batch_t **out);
+
 }  // namespace rsb
 
 extern "C" {
 
 int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *statuses, rs_batch_t **out) {
+  return batch_create(items, n_items, flags, nullptr, statuses, out);
+}
+
+int rs_batch_create_configured(const rs_batch_item *items, size_t n_items, int flags, const int *configs,
+                               int *statuses, rs_batch_t **out) {
+  return batch_create(items, n_items, flags, configs, statuses, out);
+}
+
+int rs_tuning_config_count(void) { return kTuneConfigCount; }
+
+int rs_tuning_features(void) { return kTuneFeatures; }
+
+int rs_tuning_config(int index, int *route, int *p0, int *p1) {
+  if (index < 0 || index >= kTuneConfigCount) return RS_ERR_INVALID_ARGUMENT;
+  if (route) *route = kTuneConfigs[index].route;
+  if (p0) *p0 = kTuneConfigs[index].p0;
+  if (p1) *p1 = kTuneConfigs[index].p1;
+  return RS_OK;
+}
+
+int rs_batch_choose(const rs_batch_item *items, size_t n_items, rs_mlp_t *model, int *configs) {
+  if (!model || !configs || (!items && n_items)) return RS_ERR_INVALID_ARGUMENT;
+  int n_in = 0, n_out = 0;
+  RSB_TRY(rs_mlp_dims(model, &n_in, nullptr, &n_out));
+  if (n_in != kTuneFeatures || n_out != kTuneConfigCount) return RS_ERR_INVALID_ARGUMENT;
+  // Encode items with a compiled kernel, grouped by shape and row alignment: each group
+  // is one launch of the batch, so it takes one configuration.
+  std::map<std::pair<const Gen8 *, bool>, std::vector<size_t>> groups;
+  for (size_t i = 0; i < n_items; i++) {
+    configs[i] = -1;
+    const rs_batch_item &it = items[i];
+    if (!it.codec || !it.d_rows || it.op != RS_BATCH_ENCODE || it.row_len == 0 || it.row_stride < it.row_len)
+      continue;
+    if (!it.codec->gen->fft || it.codec->route.load() != 0) continue;
+    groups[{it.codec->gen.get(), rows_aligned(it)}].push_back(i);
+  }
+  std::vector<float> x;
+  for (auto &kv : groups) {
+    const Gen8 &g = *kv.first.first;
+    for (size_t i : kv.second) {
+      float f[kTuneFeatures];
+      tune_features(g.k, g.m, items[i].row_len, 0, tune_batch(g.k, g.m, items[i].row_len, kv.second.size()),
+                    kv.first.second, f);
+      x.insert(x.end(), f, f + kTuneFeatures);
+    }
+  }
+  const size_t rows = x.size() / kTuneFeatures;
+  if (!rows) return RS_OK;
+  std::vector<float> pred(rows * kTuneConfigCount);
+  float *d = nullptr;
+  RSB_CU(cudaMalloc(&d, (x.size() + pred.size()) * sizeof(float)));
+  int st = RS_OK;
+  if (cudaMemcpy(d, x.data(), x.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+    st = RS_ERR_CUDA;
+  if (!st) st = rs_mlp_predict(model, d, (int)rows, d + x.size());
+  if (!st && cudaMemcpy(pred.data(), d + x.size(), pred.size() * sizeof(float), cudaMemcpyDeviceToHost) !=
+                 cudaSuccess)
+    st = RS_ERR_CUDA;
+  cudaFree(d);
+  if (st) return st;
+  // Per group: the applicable configuration with the least predicted total time (the
+  // model predicts log time per stripe's launch). The batch's matrix launch has one tile
+  // shape, so the matrix route is represented by configuration 0. The group keeps the
+  // library's automatic choice unless the model predicts a clear gain over it
+  // (kTrustGain): the model was fitted on uniform launches and a batch's launch groups
+  // are ragged, where a small predicted gain is within its error (measured on the
+  // 10,000-stripe mixed batch: unguarded choices lost 6-7% against the automatic ones,
+  // which were within 0.3% of the exhaustive best there).
+  constexpr double kTrustGain = 0.10;
+  size_t row = 0;
+  for (auto &kv : groups) {
+    const FftShape &sh = *kv.first.first->fft;
+    const int auto_cfg = fft_auto_config(sh, kv.first.second);
+    double best = 0, at_auto = 0;
+    int pick = -1;
+    for (int c = 0; c < kTuneConfigCount; c++) {
+      const TuneConfig &tc = kTuneConfigs[c];
+      const bool ok = tc.route == kTuneMatrix ? tc.p0 == 0 : tc.route == kTuneFft ? !sh.gen : sh.gen;
+      if (!ok) continue;
+      double total = 0;
+      for (size_t r = 0; r < kv.second.size(); r++) total += std::exp((double)pred[(row + r) * kTuneConfigCount + c]);
+      if (c == auto_cfg) at_auto = total;
+      if (pick < 0 || total < best) {
+        best = total;
+        pick = c;
+      }
+    }
+    if (auto_cfg >= 0 && best > (1.0 - kTrustGain) * at_auto) pick = -1;
+    for (size_t i : kv.second) configs[i] = pick;
+    row += kv.second.size();
+  }
+  return RS_OK;
+}
+
+}  // extern "C"
+
+namespace rsb {
+
+static int batch_create(const rs_batch_item *items, size_t n_items, int flags, const int *configs, int *statuses,
+                        rs_batch_t **out) {
   if (!out || (!items && n_items)) return RS_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   std::unique_ptr<rs_batch> b(new (std::nothrow) rs_batch());
@@ -102,7 +223,7 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     std::vector<uint32_t> surv, targets;
   };
   std::map<const Gen8 *, std::vector<Recon>> recon;  // per shape
-  std::map<const FftShape *, std::vector<size_t>> fft_groups;  // compiled shape -> items
+  std::map<FftKey, std::vector<size_t>> fft_groups;  // compiled shape and configuration -> items
   struct Regen {
     size_t item;
     std::vector<uint32_t> parity;  // missing parity shard indexes
@@ -133,9 +254,29 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     }
     const size_t n = g.k + g.m;
     if (it.op == RS_BATCH_ENCODE) {
+      const int cfg = configs ? configs[i] : -1;
+      if (cfg < -1 || cfg >= kTuneConfigCount) {
+        status[i] = RS_ERR_INVALID_ARGUMENT;
+        continue;
+      }
+      if (cfg >= 0 && !(flags & RS_BATCH_MATRIX_ONLY)) {
+        // An explicit configuration: the matrix route, or the shape's compiled kernel
+        // with this launch configuration (an error where the shape has no such kernel).
+        const TuneConfig &tc = kTuneConfigs[cfg];
+        if (tc.route == kTuneMatrix) {
+          matrix_encodes.push_back(i);
+        } else if (g.fft && (tc.route == kTuneGen) == g.fft->gen) {
+          fft_groups[{g.fft, tc.route == kTuneFft ? tc.p0 : -1, tc.route == kTuneFft ? tc.p1 : -1}].push_back(i);
+        } else {
+          status[i] = RS_ERR_INVALID_ARGUMENT;
+          continue;
+        }
+        b->bytes += n * it.row_len;
+        continue;
+      }
       b->bytes += n * it.row_len;
       if (!(flags & RS_BATCH_MATRIX_ONLY) && use_fft8(it.codec, it.row_len))
-        fft_groups[g.fft].push_back(i);
+        fft_groups[{g.fft, -1, -1}].push_back(i);
       else
         matrix_encodes.push_back(i);
       continue;
@@ -264,6 +405,7 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
     size_t off, n;
     uint64_t groups;
     bool unaligned;
+    int wide, variant;
   };
   std::vector<FftGroupOff> fgo;
   std::vector<std::vector<FftItem>> fft_host;
@@ -276,14 +418,15 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
       align |= reinterpret_cast<uintptr_t>(it.d_rows) | it.row_stride;
       FftItem f{};
       f.in_base = it.d_rows;
-      f.out_base = it.d_rows + (size_t)kv.first->k * it.row_stride;
+      f.out_base = it.d_rows + (size_t)kv.first.shape->k * it.row_stride;
       f.row_stride = it.row_stride;
       f.len = it.row_len;
       f.group_begin = g0;
       g0 += (it.row_len + 31) / 32;
       v.push_back(f);
     }
-    fgo.push_back({kv.first, ar.put(v.data(), v.size() * sizeof(FftItem)), v.size(), g0, (align & 15) != 0});
+    fgo.push_back({kv.first.shape, ar.put(v.data(), v.size() * sizeof(FftItem)), v.size(), g0, (align & 15) != 0,
+                   kv.first.wide, kv.first.variant});
     b->fft_items += v.size();
     fft_host.push_back(std::move(v));
   }
@@ -363,8 +506,8 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
   RSB_CU(cudaStreamSynchronize(b->stream));
 
   for (auto &f : fgo)
-    b->ffts.push_back({f.shape, reinterpret_cast<const FftItem *>(base + f.off), (uint32_t)f.n,
-                       f.groups, nullptr, f.unaligned});
+    b->ffts.push_back({f.shape, reinterpret_cast<const FftItem *>(base + f.off), (uint32_t)f.n, f.groups, nullptr,
+                       f.unaligned, f.wide, f.variant});
   for (auto &f : rgo)
     b->regens.push_back({f.shape, reinterpret_cast<const FftItem *>(base + f.off), (uint32_t)f.n, f.groups,
                          reinterpret_cast<const uint32_t *>(base + f.mask_off), f.unaligned});
@@ -402,6 +545,10 @@ int rs_batch_create(const rs_batch_item *items, size_t n_items, int flags, int *
   *out = b.release();
   return RS_OK;
 }
+
+}  // namespace rsb
+
+extern "C" {
 
 int rs_batch_launch(rs_batch_t *b, void *stream) {
   if (!b) return RS_ERR_INVALID_ARGUMENT;

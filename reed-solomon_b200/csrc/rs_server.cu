@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -44,6 +45,7 @@
 #include "kernels_matrix.cuh"
 #include "kernels_plan.cuh"
 #include "runtime.hpp"
+#include "tuning.hpp"
 
 namespace rsb {
 
@@ -167,6 +169,9 @@ struct rs_server {
 
   std::unordered_map<uint64_t, std::unique_ptr<Table>> tables;
   uint8_t fft_route[8][32] = {};  // [log2 K - 1][log2 bytes]: 0 auto, 1 matrix, 2 FFT
+  // The cost model's FFT launch configuration per (shape, alignment, row-bytes and
+  // group-size buckets), filled on first use (scheduler thread only).
+  std::map<uint64_t, std::pair<int, int>> fft_cfg;
 
   std::mutex mu;  // queue, completions, counters
   std::condition_variable cv_work, cv_done;
@@ -446,6 +451,45 @@ static int mark_table(const Req &q, cudaStream_t st) {
   return RS_OK;
 }
 
+// The launch configuration of one FFT launch group from the server's cost model (none:
+// the library's automatic choice): the FFT configuration with the least predicted
+// total time for `count` stripes of (K, K) with rows of about `bytes` bytes, where that
+// is predicted at least 10% faster than the automatic choice (as rs_batch_choose).
+// Decisions are cached per (K, alignment, half-octave of bytes, octave of count): one
+// model evaluation per new bucket, on the scheduler thread.
+static std::pair<int, int> fft_config(rs_server *s, const FftShape &sh, size_t bytes, size_t count, bool aligned) {
+  if (!s->cfg.model || sh.gen) return {-1, -1};
+  const int lb = (int)std::lround(2.0 * std::log2((double)std::max<size_t>(bytes, 1)));
+  const int lc = (int)std::lround(std::log2((double)std::max<size_t>(count, 1)));
+  const uint64_t key = ((uint64_t)sh.k << 32) | ((uint64_t)aligned << 24) | ((uint64_t)lb << 8) | (uint64_t)lc;
+  auto it = s->fft_cfg.find(key);
+  if (it != s->fft_cfg.end()) return it->second;
+  std::pair<int, int> pick{-1, -1};
+  float x[kTuneFeatures], *d = nullptr;
+  const size_t row = (size_t)std::exp2(lb / 2.0);
+  tune_features(sh.k, sh.m, row, 0, tune_batch(sh.k, sh.m, row, (size_t)1 << lc), aligned, x);
+  std::vector<float> pred(kTuneConfigCount);
+  if (cudaMalloc(&d, sizeof(float) * (kTuneFeatures + kTuneConfigCount)) == cudaSuccess) {
+    if (cudaMemcpy(d, x, sizeof x, cudaMemcpyHostToDevice) == cudaSuccess &&
+        rs_mlp_predict(s->cfg.model, d, 1, d + kTuneFeatures) == RS_OK &&
+        cudaMemcpy(pred.data(), d + kTuneFeatures, sizeof(float) * kTuneConfigCount, cudaMemcpyDeviceToHost) ==
+            cudaSuccess) {
+      float best = 0;
+      for (int c = 0; c < kTuneConfigCount; c++)
+        if (kTuneConfigs[c].route == kTuneFft && (pick.first < 0 || pred[c] < best)) {
+          best = pred[c];
+          pick = {kTuneConfigs[c].p0, kTuneConfigs[c].p1};
+        }
+      const int auto_cfg = fft_auto_config(sh, aligned);
+      if (auto_cfg >= 0 && std::exp((double)best) > 0.9 * std::exp((double)pred[auto_cfg])) pick = {-1, -1};
+    }
+    cudaFree(d);
+  }
+  cudaGetLastError();  // a failed evaluation leaves the automatic choice
+  s->fft_cfg[key] = pick;
+  return pick;
+}
+
 // One GF(2^8) launch group: tables, plans, then one FFT launch per K and one ragged
 // matrix launch for the rest.
 static int enqueue_gf8(rs_server *s, Group &g, cudaStream_t st) {
@@ -568,8 +612,9 @@ static int enqueue_gf8(rs_server *s, Group &g, cudaStream_t st) {
     uint64_t groups = v.back().group_begin + (v.back().len + 31) / 32;
     uintptr_t align = 0;
     for (const FftItem &f : v) align |= reinterpret_cast<uintptr_t>(f.in_base) | f.row_stride;
-    RSB_TRY(launch_fft8_items(*kv.first, reinterpret_cast<const FftItem *>(gd + off),
-                              (uint32_t)v.size(), groups, st, nullptr, (align & 15) != 0));
+    const std::pair<int, int> cfg = fft_config(s, *kv.first, groups * 32 / v.size(), v.size(), (align & 15) == 0);
+    RSB_TRY(launch_fft8_items(*kv.first, reinterpret_cast<const FftItem *>(gd + off), (uint32_t)v.size(), groups, st,
+                              nullptr, (align & 15) != 0, cfg.first, cfg.second));
     g.launches++;
     off = up256(off + v.size() * sizeof(FftItem));
   }

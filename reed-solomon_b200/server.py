@@ -29,7 +29,8 @@ class Completion(ctypes.Structure):
 
 class Config(ctypes.Structure):
     _fields_ = [("arena_bytes", ctypes.c_size_t), ("pinned_bytes", ctypes.c_size_t), ("slots", ctypes.c_int),
-                ("streams", ctypes.c_int), ("max_batch", ctypes.c_int), ("lookahead", ctypes.c_int)]
+                ("streams", ctypes.c_int), ("max_batch", ctypes.c_int), ("lookahead", ctypes.c_int),
+                ("model", ctypes.c_void_p)]
 
 
 class Stats(ctypes.Structure):
@@ -42,9 +43,13 @@ class Stats(ctypes.Structure):
 class Server:
     """rs_server_create with the given limits (0 = library default)."""
 
-    def __init__(self, arena_bytes=1 << 30, slots=64, streams=4, max_batch=64, lookahead=0, pinned_bytes=0):
+    def __init__(self, arena_bytes=1 << 30, slots=64, streams=4, max_batch=64, lookahead=0, pinned_bytes=0,
+                 model=None):
         self._L = _lib.load()
-        cfg = Config(arena_bytes, pinned_bytes, slots, streams, max_batch, lookahead)
+        # model: a tuner.CostModel choosing FFT launch shapes (kept alive with the server).
+        self._model = model
+        cfg = Config(arena_bytes, pinned_bytes, slots, streams, max_batch, lookahead,
+                     model._h.value if model is not None else None)
         h = ctypes.c_void_p()
         _check(self._L.rs_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

@@ -15,6 +15,7 @@ Candidates (GF(2^8)):
 """
 import ctypes
 import math
+import os
 
 import numpy as np
 
@@ -24,7 +25,10 @@ from .coder import ReedSolomon, _check
 CONFIGS = [("matrix", 0), ("matrix", 1), ("matrix", 2), ("matrix", 3),
            ("fft", (0, 0)), ("fft", (0, 1)), ("fft", (1, 0)), ("fft", (1, 1)),
            ("fft", (0, 2)), ("fft", (1, 2)), ("fft", (0, 3)), ("fft", (1, 3)), ("gen", 0)]
-N_FEATURES = 5
+N_FEATURES = 6
+MAX_BATCH_LOG2 = 9  # stripes per timed launch: 1 .. 512 (the library clamps the feature there)
+MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cost_model.rsmlp")
+TIMINGS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cost_model_timings.npz")
 FFT_K = (2, 4, 8, 16, 32, 64, 128)
 GEN_SHAPES = ((7, 13), (10, 10), (14, 14), (18, 6), (20, 12), (4, 2), (6, 3), (8, 4), (10, 4), (12, 4),
               (16, 4), (17, 3))
@@ -37,9 +41,15 @@ class Workload:
     def __init__(self, k, m, shard_bytes, erasures=0, batch=1):
         self.k, self.m, self.shard_bytes, self.erasures, self.batch = k, m, shard_bytes, erasures, batch
 
+    def aligned(self):
+        """Rows are packed shard_bytes apart, so they are 16-byte aligned iff that is."""
+        return self.shard_bytes % 16 == 0
+
     def features(self):
+        """As the library computes them (tuning.hpp tune_features)."""
+        batch = min(max(self.batch, 1), 1 << MAX_BATCH_LOG2)
         return [math.log2(self.k) / 8.0, math.log2(self.m) / 8.0, math.log2(self.shard_bytes) / 20.0,
-                self.erasures / max(self.m, 1), math.log2(self.batch) / 8.0]
+                self.erasures / max(self.m, 1), math.log2(batch) / 8.0, 0.0 if self.aligned() else 1.0]
 
     def bytes(self):
         return self.batch * self.shard_bytes * (self.k + (self.erasures or self.m))
@@ -139,10 +149,11 @@ def exhaustive(w, reps=3, seed=0):
     return t
 
 
-def sample_workloads(n, seed, max_bytes=96 << 20):
+def sample_workloads(n, seed, max_bytes=64 << 20):
     """GF(2^8) workloads spread like the serving mix: k log-uniform, shard bytes
-    log-uniform 512 B .. 1 MiB, a quarter reconstruct; (K,K) power-of-two shapes
-    over-sampled so the FFT candidates are exercised."""
+    log-uniform 512 B .. 1 MiB (half of them rounded to a multiple of 16, so that rows
+    packed back to back are 16-byte aligned), a quarter reconstruct; (K,K) power-of-two
+    shapes over-sampled so the FFT candidates are exercised."""
     rng = np.random.default_rng(seed)
     out = []
     while len(out) < n:
@@ -158,8 +169,10 @@ def sample_workloads(n, seed, max_bytes=96 << 20):
             if k + m > 256 or m < 1:
                 continue
         shard = int(math.exp(rng.uniform(math.log(512), math.log(1 << 20))))
+        if rng.random() < 0.5:  # half on 16-byte aligned rows (as separately allocated shards are)
+            shard = max(16, shard // 16 * 16)
         erasures = int(rng.integers(1, m + 1)) if rng.random() < 0.25 else 0
-        batch = int(2 ** rng.integers(0, 7))
+        batch = int(2 ** rng.integers(0, MAX_BATCH_LOG2 + 1))
         w = Workload(k, m, shard, erasures, batch)
         while w.bytes() > max_bytes and w.batch > 1:
             w.batch //= 2
@@ -178,11 +191,17 @@ def collect(workloads, reps=3):
 class CostModel:
     """FP32 MLP on the GPU (rs_mlp_*): features -> log(ms) per configuration."""
 
-    def __init__(self, hidden=64, seed=1):
+    def __init__(self, hidden=64, seed=1, path=None):
         self._L = _lib.load()
         h = ctypes.c_void_p()
-        _check(self._L.rs_mlp_create(N_FEATURES, hidden, len(CONFIGS), seed, ctypes.byref(h)))
+        if path is not None:
+            _check(self._L.rs_mlp_load(os.fsencode(path), ctypes.byref(h)))
+        else:
+            _check(self._L.rs_mlp_create(N_FEATURES, hidden, len(CONFIGS), seed, ctypes.byref(h)))
         self._h = h
+
+    def save(self, path):
+        _check(self._L.rs_mlp_save(self._h, os.fsencode(path)))
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -252,6 +271,24 @@ class CostModel:
         P = self.predict(X)
         P = np.where(np.isfinite(T), P, np.inf)
         return P.argmin(axis=1)
+
+
+def shipped_model():
+    """The cost model trained on this library's autotuner timings (cost_model.rsmlp,
+    made by `bench.py --workload tuner --save-model`), or None when absent."""
+    return CostModel(path=MODEL_PATH) if os.path.exists(MODEL_PATH) else None
+
+
+def library_configs():
+    """The library's configuration table (rs_tuning_config), as CONFIGS spells it."""
+    L = _lib.load()
+    out = []
+    for i in range(L.rs_tuning_config_count()):
+        r, a, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(L.rs_tuning_config(i, ctypes.byref(r), ctypes.byref(a), ctypes.byref(b)))
+        out.append(("matrix", a.value) if r.value == 0 else ("fft", (a.value, b.value)) if r.value == 1
+                   else ("gen", 0))
+    return out
 
 
 DEFAULT_FFT = {2: (0, 0), 4: (0, 1), 8: (0, 1), 16: (0, 1), 32: (0, 3), 64: (0, 3), 128: (1, 3)}

@@ -13,7 +13,7 @@ import time
 import numpy as np
 
 from . import _lib
-from .coder import ENCODE, MATRIX_ONLY, RECONSTRUCT, Batch, ReedSolomon, ReedSolomon16
+from .coder import ENCODE, MATRIX_ONLY, RECONSTRUCT, Batch, ReedSolomon, ReedSolomon16, _dev_ptr
 
 MIXED_SHAPES = [(7, 13), (10, 10), (14, 14), (16, 16), (18, 6), (32, 32), (20, 12), (64, 64), (128, 128)]
 
@@ -100,7 +100,7 @@ def stripes_sweep(shapes=((32, 32), (16, 16)), sizes=(4096, 65536, 1 << 20), n_s
 
 # ---- mixed batch: 10,000 stripes of nine shapes, 25% reconstruct ----
 
-def mixed_batch(n=10000, seed=3, reps=5, packed=False):
+def mixed_batch(n=10000, seed=3, reps=5, packed=False, tuned_compare=True):
     """Batched+tuned (one graph: one compiled-kernel launch per FFT or generator shape + one
     ragged matrix launch) against
     the plain path (one matrix-kernel call per stripe; reconstructs build their decode
@@ -179,13 +179,74 @@ def mixed_batch(n=10000, seed=3, reps=5, packed=False):
     t_batched_matrix = _time(batch_m.launch, reps, warmup=2)
     for c in codecs.values():
         c.set_route("auto")
+    tuned = tuned_vs_exhaustive(items, t_batched, reps) if tuned_compare else {}
     return {"stripes": n, "bytes": nbytes, "batched_gbs": nbytes / t_batched / 1e9,
             "batched_ms": t_batched * 1e3, "batched_launches": stats["launches"],
             "fft_items": stats["fft_items"], "matrix_items": stats["matrix_items"],
             "batched_matrix_only_gbs": nbytes / t_batched_matrix / 1e9,
             "plain_gbs": nbytes / t_plain / 1e9, "plain_ms": t_plain * 1e3, "plain_launches": plain_launches,
             "batched_over_plain": t_plain / t_batched, "create_s": create_s,
-            "batched_incl_create_over_plain": t_plain / (t_batched + create_s)}
+            "batched_incl_create_over_plain": t_plain / (t_batched + create_s),
+            **tuned, **({"exhaustive_gbs": nbytes / tuned["exhaustive_ms"] * 1e3 / 1e9} if tuned else {}),
+            **({"model_gbs": nbytes / tuned["model_ms"] * 1e3 / 1e9} if "model_ms" in tuned else {})}
+
+
+def tuned_vs_exhaustive(items, t_default, reps):
+    """The batch's launch configurations three ways: the library's defaults (t_default,
+    timed by the caller), the shipped cost model's choice (rs_batch_choose), and the
+    exhaustive best: every launch group (encodes of one compiled shape and row
+    alignment) timed alone under each applicable configuration, the fastest kept per
+    group. Returns the replay times and the regrets against the exhaustive best."""
+    from . import tuner
+
+    model = tuner.shipped_model()
+    out = {}
+    groups = {}
+    for i, (codec, rows, stride, S, op, present) in enumerate(items):
+        sh = (codec.data_shard_count(), codec.parity_shard_count())
+        if op != ENCODE or (sh not in tuner.GEN_SHAPES and not (sh[0] == sh[1] and sh[0] in tuner.FFT_K)):
+            continue
+        aligned = (_dev_ptr(rows) | stride) % 16 == 0
+        groups.setdefault((sh, aligned), []).append(i)
+    best_cfg = [-1] * len(items)
+    tried = 0
+    for (sh, aligned), idx in groups.items():
+        sub = [items[i] for i in idx]
+        gen = sh in tuner.GEN_SHAPES
+        cands = [c for c, (route, _) in enumerate(tuner.CONFIGS)
+                 if (route == "matrix" and c == 0) or (route == "gen" and gen) or (route == "fft" and not gen)]
+        times = []
+        for c in cands:
+            b = Batch(sub, configs=[c] * len(sub))
+            times.append(_time(b.launch, reps, warmup=1))
+            tried += 1
+        pick = cands[int(np.argmin(times))]
+        for i in idx:
+            best_cfg[i] = pick
+    t_exh = _time(Batch(items, configs=best_cfg).launch, reps, warmup=2)
+    out["exhaustive_ms"] = t_exh * 1e3
+    out["exhaustive_groups"] = len(groups)
+    out["exhaustive_timed_configs"] = tried
+    out["regret_default"] = t_default / t_exh - 1.0
+    if model is not None:
+        bm = Batch(items, model=model)
+        t_model = _time(bm.launch, reps, warmup=2)
+        out["model_ms"] = t_model * 1e3
+        out["regret_model"] = t_model / t_exh - 1.0
+        def resolved(sh, aligned, cfg):  # -1: the automatic choice, as its table entry
+            if cfg >= 0:
+                return cfg
+            if sh in tuner.GEN_SHAPES:
+                return tuner.CONFIGS.index(("gen", 0))
+            table = tuner.DEFAULT_FFT if aligned or sh[0] < 16 else tuner.UNALIGNED_FFT
+            return tuner.CONFIGS.index(("fft", table[sh[0]]))
+
+        out["model_groups_matching_exhaustive"] = sum(
+            1 for (sh, al), idx in groups.items() if resolved(sh, al, bm.configs[idx[0]]) == best_cfg[idx[0]])
+        out["groups"] = [{"shape": list(sh), "aligned": al, "stripes": len(idx),
+                          "model": resolved(sh, al, bm.configs[idx[0]]), "model_kept_automatic": bm.configs[idx[0]] < 0,
+                          "exhaustive": best_cfg[idx[0]]} for (sh, al), idx in groups.items()]
+    return out
 
 
 # ---- ReedSolomon16: (1024,1024) and (4096,12288), 2 KiB shards ----
@@ -259,7 +320,8 @@ def rs16_shapes(shapes=((1024, 1024, 64), (4096, 12288, 2)), S=2048, seed=4, rep
 
 # ---- autotuner and learned cost model ----
 
-def tuner_regret(n_workloads=1500, seed=11, train_frac=0.8, max_bytes=32 << 20, epochs=300):
+def tuner_regret(n_workloads=1500, seed=11, train_frac=0.8, max_bytes=64 << 20, epochs=300, save_model=None,
+                 save_timings=None):
     """Exhaustive tuning of sampled GF(2^8) workloads (every applicable route / tile,
     timed on the GPU), the FP32 MLP cost model trained on most of them by the library's
     CUDA kernels, and its regret on the held-out rest against exhaustive tuning, beside
@@ -275,6 +337,11 @@ def tuner_regret(n_workloads=1500, seed=11, train_frac=0.8, max_bytes=32 << 20, 
     t1 = time.perf_counter()
     hist = m.fit(X[:n_tr], T[:n_tr], epochs=epochs, lr=3e-3, batch=256)
     train_s = time.perf_counter() - t1
+    if save_model:  # the model whose held-out regret is reported below
+        m.save(save_model)
+    if save_timings:
+        np.savez_compressed(save_timings, X=X, T=T, train=n_tr, seed=seed,
+                            configs=np.array([str(c) for c in tuner.CONFIGS]))
     te = slice(n_tr, len(work))
     choice = m.choose(X[te], T[te])
     default = tuner.default_choice(work[te], T[te])
@@ -313,13 +380,15 @@ def poisson_requests(count, rate, seed):
 
 
 def serve_poisson(count=400, rate=50000.0, seed=5, arena_bytes=4 << 30, slots=64, streams=16, max_batch=64,
-                  lookahead=64, route_hints=None):
+                  lookahead=64, route_hints=None, tuned=True):
     """Submits `count` requests at their Poisson arrival times (device-resident stripes
     carved from one synthetic pool; overlapping stripes share bytes, which changes no
     timing because the arithmetic is data-independent) and reports latency from arrival
-    to completion, and throughput over the whole run."""
+    to completion, and throughput over the whole run. With `tuned` the server's FFT
+    launch shapes come from the shipped cost model."""
     import torch
 
+    from . import tuner
     from .server import Server
 
     reqs = poisson_requests(count, rate, seed)
@@ -331,7 +400,9 @@ def serve_poisson(count=400, rate=50000.0, seed=5, arena_bytes=4 << 30, slots=64
     for r in reqs:
         span = (r["k"] + r["m"]) * r["row_len"]
         r["rows"] = base + (int(rng.integers(0, biggest - span + 1)) & ~255)
-    srv = Server(arena_bytes=arena_bytes, slots=slots, streams=streams, max_batch=max_batch, lookahead=lookahead)
+    model = tuner.shipped_model() if tuned else None
+    srv = Server(arena_bytes=arena_bytes, slots=slots, streams=streams, max_batch=max_batch, lookahead=lookahead,
+                 model=model)
     for k, log2b, route in (route_hints or []):
         srv.set_fft_route(k, log2b, route)
     torch.cuda.synchronize()

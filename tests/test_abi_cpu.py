@@ -139,3 +139,40 @@ def test_fft_tuning_hooks_and_automatic_choice(rsb):
     assert L.rs_set_fft_lanes(128, -1) == wide
     assert L.rs_set_fft_lanes(128, 2) == -1
     assert L.rs_set_fft_lanes(14, 0) == -1
+
+
+def test_tuning_configurations_match_the_tuner(rsb):
+    """The library's configuration table (the cost model's output order) is the one the
+    Python tuner times, and the model reads the six features it computes."""
+    from reed_solomon_b200 import tuner
+
+    assert tuner.library_configs() == tuner.CONFIGS
+    assert rsb.load().rs_tuning_features() == tuner.N_FEATURES
+
+
+def test_shipped_cost_model_file(rsb):
+    """cost_model.rsmlp: the magic, then 6 inputs, 64 hidden, 13 outputs, then exactly
+    the network's float32 parameters, all finite."""
+    import struct
+
+    import numpy as np
+
+    from reed_solomon_b200 import tuner
+
+    blob = open(tuner.MODEL_PATH, "rb").read()
+    assert blob[:8] == b"RSMLP\x00\x00\x01"
+    n_in, hidden, n_out = struct.unpack("<3i", blob[8:20])
+    assert (n_in, hidden, n_out) == (tuner.N_FEATURES, 64, len(tuner.CONFIGS))
+    n_params = n_in * hidden + hidden + 2 * (hidden * hidden + hidden) + hidden * n_out + n_out
+    params = np.frombuffer(blob[20:], dtype="<f4")
+    assert params.size == n_params and np.all(np.isfinite(params))
+
+
+def test_mlp_load_rejects_other_files(rsb, tmp_path):
+    import ctypes
+
+    bad = tmp_path / "not_a_model.bin"
+    bad.write_bytes(b"RSMLP\x00\x00\x02" + b"\x00" * 64)
+    h = ctypes.c_void_p()
+    assert rsb.load().rs_mlp_load(str(bad).encode(), ctypes.byref(h)) == 102
+    assert rsb.load().rs_mlp_load(str(tmp_path / "missing").encode(), ctypes.byref(h)) == 102

@@ -83,8 +83,15 @@ def _background(O, count, seed):
     return specs
 
 
-def test_alone_equals_in_mix(gpu, O):
-    srv = gpu.Server(arena_bytes=256 << 20, slots=32, streams=4, max_batch=16, lookahead=8)
+@pytest.mark.parametrize("tuned", [False, True])
+def test_alone_equals_in_mix(gpu, O, tuned):
+    """With tuned=True the server's cost model (the shipped one) picks the FFT launch
+    groups' launch shapes; results must not change."""
+    from reed_solomon_b200 import tuner
+
+    model = tuner.shipped_model() if tuned else None
+    assert model is not None or not tuned
+    srv = gpu.Server(arena_bytes=256 << 20, slots=32, streams=4, max_batch=16, lookahead=8, model=model)
     alone = []
     for i, spec in enumerate(PROBES):
         req, expect = _make(O, spec, seed=10 + i)
