@@ -266,6 +266,35 @@ int rs_batch_stats(const rs_batch_t *batch, size_t *launches, size_t *fft_items,
                    size_t *matrix_items, uint64_t *bytes);
 void rs_batch_free(rs_batch_t *batch);
 
+/* ---- persistent work queue: one long-running launch fed while it runs ----
+ * No counterpart in the reference. A session starts one persistent kernel (a captured
+ * graph, replayed per session) and the host then pushes stripes (rs_batch_item: any
+ * GF(2^8) shape, shard length and erasure pattern, validated as rs_batch_create does;
+ * each item's status as its single-stripe call would return it) while it runs; every
+ * stripe is cut into units of at most 16 matrix-kernel blocks, and the kernel's CTAs
+ * take units in order as they are published. Every device wait is bounded: a CTA that
+ * waits longer than timeout_ns (global timer; 0 = 1 s) for a unit that is not published
+ * and not closed gives up, and the session ends with RS_ERR_TIMEOUT (the device stays
+ * usable; units published before were run). Reconstruct units use decode rows built on
+ * the host and copied to the queue's device arena (arena_bytes; 0 = 64 MiB) before they
+ * are published. All work runs on the matrix route. */
+typedef struct rs_queue rs_queue_t;
+int rs_queue_create(size_t max_units, size_t arena_bytes, uint64_t timeout_ns, rs_queue_t **out);
+/* Begins a session (RS_ERR_INVALID_ARGUMENT while one runs). */
+int rs_queue_start(rs_queue_t *queue);
+/* Appends and publishes stripes; RS_ERR_TOO_LARGE when the session's units or arena
+ * would overflow (nothing is published then). The rows must stay valid until the
+ * session ends. */
+int rs_queue_push(rs_queue_t *queue, const rs_batch_item *items, size_t n_items, int *statuses);
+/* Units finished by the device so far and units published in this session. */
+int rs_queue_progress(rs_queue_t *queue, uint64_t *done_units, uint64_t *published_units);
+/* Closes the session (nothing more will be pushed), waits for the kernel and returns
+ * its status: 0, or RS_ERR_TIMEOUT when a wait gave up before the close. */
+int rs_queue_finish(rs_queue_t *queue);
+/* Waits for the kernel without closing (it ends when a wait gives up: RS_ERR_TIMEOUT). */
+int rs_queue_wait(rs_queue_t *queue);
+void rs_queue_free(rs_queue_t *queue);
+
 /* ---- request server: continuous batching on one GPU ----
  * No counterpart in the reference (a caller there runs one encode or reconstruct per
  * call on its own thread). A server owns a device arena, a set of streams and a

@@ -13,6 +13,7 @@ from .coder import (  # noqa: F401
     Batch,
     PreparedDecoder,
     PreparedDecoder16,
+    Queue,
     ReedSolomon,
     ReedSolomon16,
     RsError,

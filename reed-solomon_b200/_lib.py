@@ -70,6 +70,13 @@ SIGNATURES = {
     "rs_batch_launch": (_int, [_vp, _vp]),
     "rs_batch_stats": (_int, [_vp, _szp, _szp, _szp, ctypes.POINTER(ctypes.c_uint64)]),
     "rs_batch_free": (None, [_vp]),
+    "rs_queue_create": (_int, [_sz, _sz, ctypes.c_uint64, _pp]),
+    "rs_queue_start": (_int, [_vp]),
+    "rs_queue_push": (_int, [_vp, _vp, _sz, _intp]),
+    "rs_queue_progress": (_int, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    "rs_queue_finish": (_int, [_vp]),
+    "rs_queue_wait": (_int, [_vp]),
+    "rs_queue_free": (None, [_vp]),
     "rs_server_create": (_int, [_vp, _pp]),
     "rs_server_submit": (_int, [_vp, _vp, _sz, _intp]),
     "rs_server_poll": (_int, [_vp, _vp, _sz, _szp, _int]),

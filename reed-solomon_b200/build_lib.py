@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "librsb200.so")
-SOURCES = ["rs_abi.cu", "rs16_abi.cu", "rs_batch.cu", "mlp.cu", "rs_noalloc.cu", "rs_frame.cu", "rs_server.cu", "fft16.cu", "fft_k_small.cu", "fft_k16.cu", "fft_k32.cu",
+SOURCES = ["rs_abi.cu", "rs16_abi.cu", "rs_batch.cu", "mlp.cu", "rs_noalloc.cu", "rs_frame.cu", "rs_queue.cu", "rs_server.cu", "fft16.cu", "fft_k_small.cu", "fft_k16.cu", "fft_k32.cu",
            "fft_k64.cu", "fft_k128.cu", "gen_k.cu", "gen_k_more.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

@@ -479,6 +479,72 @@ ENCODE, RECONSTRUCT, RECONSTRUCT_DATA = 0, 1, 2
 MATRIX_ONLY, NO_GRAPH = 1, 2
 
 
+def _batch_items(items):
+    """rs_batch_item array for (codec, rows, row_stride, row_len, op, present) tuples, and
+    the flag arrays it points into (keep them alive while it is used)."""
+    arr = (_BatchItem * max(len(items), 1))()
+    keep = []
+    for i, (codec, rows, stride, row_len, op, present) in enumerate(items):
+        arr[i].codec = codec._h.value
+        arr[i].d_rows = _dev_ptr(rows)
+        arr[i].row_stride = stride
+        arr[i].row_len = row_len
+        arr[i].op = op
+        if present is not None:
+            f, fp = _flags(present)
+            keep.append(f)
+            arr[i].present = fp
+    return arr, keep
+
+
+class Queue:
+    """Persistent work queue (rs_queue_*): start() launches one persistent kernel; push()
+    hands it stripes (the Batch item tuples) while it runs; finish() closes the session
+    and returns its status (0, or the Timeout code 104 when a device wait gave up);
+    wait() waits without closing. Rows must stay valid until the session ends."""
+
+    def __init__(self, max_units=1 << 16, arena_bytes=0, timeout_s=1.0):
+        self._L = _lib.load()
+        h = ctypes.c_void_p()
+        _check(self._L.rs_queue_create(max_units, arena_bytes, int(timeout_s * 1e9), ctypes.byref(h)))
+        self._h = h
+        self._hold = []
+
+    def start(self):
+        self._hold = []
+        _check(self._L.rs_queue_start(self._h))
+
+    def push(self, items):
+        arr, keep = _batch_items(items)
+        st = (ctypes.c_int * max(len(items), 1))()
+        _check(self._L.rs_queue_push(self._h, arr, len(items), st))
+        self._hold.append((items, keep))
+        return list(st)[:len(items)]
+
+    def progress(self):
+        d, p = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(self._L.rs_queue_progress(self._h, ctypes.byref(d), ctypes.byref(p)))
+        return d.value, p.value
+
+    def _end(self, fn):
+        code = fn(self._h)
+        if code not in (0, 104):
+            _check(code)
+        return code
+
+    def finish(self):
+        return self._end(self._L.rs_queue_finish)
+
+    def wait(self):
+        return self._end(self._L.rs_queue_wait)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._L.rs_queue_free(h)
+            self._h = None
+
+
 class Batch:
     """A mixed batch of GF(2^8) stripes (rs_batch_create): items are tuples
     (codec, rows, row_stride, row_len, op, present) with `rows` a CUDA tensor or device
@@ -492,18 +558,7 @@ class Batch:
     def __init__(self, items, flags=0, configs=None, model=None):
         self._L = _lib.load()
         n = len(items)
-        arr = (_BatchItem * max(n, 1))()
-        self._keep = []
-        for i, (codec, rows, stride, row_len, op, present) in enumerate(items):
-            arr[i].codec = codec._h.value
-            arr[i].d_rows = _dev_ptr(rows)
-            arr[i].row_stride = stride
-            arr[i].row_len = row_len
-            arr[i].op = op
-            if present is not None:
-                f, fp = _flags(present)
-                self._keep.append(f)
-                arr[i].present = fp
+        arr, self._keep = _batch_items(items)
         self._codecs = [it[0] for it in items]
         st = (ctypes.c_int * max(n, 1))()
         h = ctypes.c_void_p()

@@ -36,20 +36,16 @@ __device__ __forceinline__ uint32_t find_item(const RaggedItem *items, uint32_t 
   return lo;
 }
 
-// Dynamic shared memory: 8 KiB constant table + up to max_rows*max_k coefficients.
+// One block of work of an item: row chunk `local / col_tiles`, column tile
+// `local % col_tiles`. R is the 8 KiB constant table (fill_rtab, filled once), C room
+// for kRowChunk x k coefficients. Every thread of the CTA calls it (it meets at
+// barriers around the coefficient table).
 template <int OUT_TILE>
-__global__ void __launch_bounds__(kThreads)
-    gf8_ragged_kernel(const RaggedItem *__restrict__ items, uint32_t n_items) {
-  extern __shared__ __align__(16) uint32_t smem[];
-  uint32_t *R = smem;
-  uint8_t *C = reinterpret_cast<uint8_t *>(smem + 2048);
-  fill_rtab(R);
-  const uint32_t it = find_item(items, n_items, blockIdx.x);
-  const RaggedItem &w = items[it];
-  const uint32_t local = blockIdx.x - w.block_begin;
+__device__ __forceinline__ void ragged_block(const RaggedItem &w, uint32_t local, const uint32_t *R, uint8_t *C) {
   const uint32_t chunk = local / w.col_tiles, tile = local % w.col_tiles;
   const uint32_t k = w.k;
   const uint32_t g0 = chunk * kRowChunk, g_end = min(w.rows, g0 + kRowChunk);
+  __syncthreads();  // the previous block's readers of C are done
   for (uint32_t t = threadIdx.x; t < (g_end - g0) * k; t += kThreads) C[t] = w.coeffs[g0 * k + t];
   __syncthreads();
   const uint64_t col = ((uint64_t)tile * kThreads + threadIdx.x) * kBytesPerThread;
@@ -90,6 +86,19 @@ __global__ void __launch_bounds__(kThreads)
       }
     }
   }
+}
+
+// Dynamic shared memory: 8 KiB constant table + up to max_rows*max_k coefficients.
+template <int OUT_TILE>
+__global__ void __launch_bounds__(kThreads)
+    gf8_ragged_kernel(const RaggedItem *__restrict__ items, uint32_t n_items) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t *R = smem;
+  uint8_t *C = reinterpret_cast<uint8_t *>(smem + 2048);
+  fill_rtab(R);
+  const uint32_t it = find_item(items, n_items, blockIdx.x);
+  const RaggedItem &w = items[it];
+  ragged_block<OUT_TILE>(w, blockIdx.x - w.block_begin, R, C);
 }
 
 }  // namespace rsb

@@ -180,6 +180,7 @@ def mixed_batch(n=10000, seed=3, reps=5, packed=False, tuned_compare=True):
     for c in codecs.values():
         c.set_route("auto")
     tuned = tuned_vs_exhaustive(items, t_batched, reps) if tuned_compare else {}
+    queue = queue_session(items, nbytes) if tuned_compare else {}
     return {"stripes": n, "bytes": nbytes, "batched_gbs": nbytes / t_batched / 1e9,
             "batched_ms": t_batched * 1e3, "batched_launches": stats["launches"],
             "fft_items": stats["fft_items"], "matrix_items": stats["matrix_items"],
@@ -188,7 +189,29 @@ def mixed_batch(n=10000, seed=3, reps=5, packed=False, tuned_compare=True):
             "batched_over_plain": t_plain / t_batched, "create_s": create_s,
             "batched_incl_create_over_plain": t_plain / (t_batched + create_s),
             **tuned, **({"exhaustive_gbs": nbytes / tuned["exhaustive_ms"] * 1e3 / 1e9} if tuned else {}),
-            **({"model_gbs": nbytes / tuned["model_ms"] * 1e3 / 1e9} if "model_ms" in tuned else {})}
+            **({"model_gbs": nbytes / tuned["model_ms"] * 1e3 / 1e9} if "model_ms" in tuned else {}), **queue}
+
+
+def queue_session(items, nbytes):
+    """The same stripes through the persistent work queue (one launch, all on the matrix
+    route): pushed in chunks of 500 while the kernel runs; host time from start to the
+    end of finish(), pushes (validation, host decode rows) included; best of two."""
+    from .coder import Queue
+
+    q = Queue(max_units=1 << 18, arena_bytes=256 << 20, timeout_s=10.0)
+    best = None
+    for _ in range(2):
+        t0 = time.perf_counter()
+        q.start()
+        for c0 in range(0, len(items), 500):
+            st = q.push(items[c0:c0 + 500])
+            assert all(x == 0 for x in st)
+        code = q.finish()
+        t = time.perf_counter() - t0
+        assert code == 0
+        best = t if best is None else min(best, t)
+    done, published = q.progress()
+    return {"queue_gbs": nbytes / best / 1e9, "queue_s": best, "queue_units": published}
 
 
 def tuned_vs_exhaustive(items, t_default, reps):
