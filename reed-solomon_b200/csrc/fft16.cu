@@ -65,10 +65,12 @@ void push_const16(std::vector<uint16_t> &cols, uint16_t c) {
   const uint8_t hi = (uint8_t)(c >> 8), lo = (uint8_t)c;
   const uint8_t k[3] = {lo, (uint8_t)(hi ^ lo), gf8_mul(hi, 32)};
   const size_t at = cols.size();
-  cols.resize(at + 16);  // three factors' 4 words each, then 4 zero words
+  cols.resize(at + 16);  // three factors' 4 words each, then the factors, then zeros
   uint16_t *o = cols.data() + at;
   for (int t = 0; t < 3; t++)
     for (int i = 0; i < 4; i++) o[t * 4 + i] = cw.w[k[t]][i];
+  o[12] = (uint16_t)(k[0] | (k[1] << 8));  // bytes 24..26: k0, k1, k2
+  o[13] = k[2];
 }
 
 uint64_t push_const(Fft16Program &p, uint16_t c) {
@@ -473,3 +475,10 @@ int fft16_run(const Fft16Program &p, const uint16_t *d_cols, uint8_t *scratch, s
 }
 
 }  // namespace rsb
+
+extern "C" int rs_set_fft16_pass(int variant) {
+  if (variant < 0 || variant > 1) return -1;
+  const int old = rsb::fft16_pass_variant();
+  rsb::fft16_pass_variant() = variant;
+  return old;
+}

@@ -263,15 +263,182 @@ __global__ void __launch_bounds__(32, 16) fft16_pass_kernel(const Fft16PassArgs 
   }
 }
 
+// ---- runtime constants through compile-time networks ----
+// A butterfly constant is known only at run time, but it is the same for every lane of
+// the warp, so each of its three GF(2^8) Karatsuba factors k can select a compiled XOR
+// network instead of being applied as 64 masked XORs: k * x = (k & 15) * x + (k & 0xF0) * x,
+// and (k & 0xF0) = (k >> 4) * alpha^4 needs no reduction, so both halves are one of 16
+// compile-time constants applied to x itself (kernels_fft.cuh mul_set / mul_acc, about
+// 10 LOP3 each against 64 masked LOP3 and 16 mask loads). The two switches live in one
+// out-of-line function with its operands in registers, so the networks exist once.
+struct Planes8 {
+  uint32_t v[8];
+};
+
+template <int J>
+__device__ __forceinline__ void nib_lo(Planes8 &t, const Planes8 &x) {
+  fftc::mul_set<(uint8_t)J>(*reinterpret_cast<fftc::Reg *>(t.v), *reinterpret_cast<const fftc::Reg *>(x.v));
+}
+template <int J>
+__device__ __forceinline__ void nib_hi(Planes8 &t, const Planes8 &x) {
+  fftc::mul_acc<(uint8_t)(J << 4)>(*reinterpret_cast<fftc::Reg *>(t.v), *reinterpret_cast<const fftc::Reg *>(x.v));
+}
+
+// k * x for a warp-uniform byte k.
+__device__ __noinline__ Planes8 mul8_rt(Planes8 x, uint32_t k) {
+  Planes8 t;
+  switch (k & 15) {
+#define RSB_NIB(j)   \
+  case j:            \
+    nib_lo<j>(t, x); \
+    break;
+    RSB_NIB(0) RSB_NIB(1) RSB_NIB(2) RSB_NIB(3) RSB_NIB(4) RSB_NIB(5) RSB_NIB(6) RSB_NIB(7)
+    RSB_NIB(8) RSB_NIB(9) RSB_NIB(10) RSB_NIB(11) RSB_NIB(12) RSB_NIB(13) RSB_NIB(14) RSB_NIB(15)
+#undef RSB_NIB
+  }
+  switch ((k >> 4) & 15) {
+#define RSB_NIB(j)   \
+  case j:            \
+    nib_hi<j>(t, x); \
+    break;
+    RSB_NIB(0) RSB_NIB(1) RSB_NIB(2) RSB_NIB(3) RSB_NIB(4) RSB_NIB(5) RSB_NIB(6) RSB_NIB(7)
+    RSB_NIB(8) RSB_NIB(9) RSB_NIB(10) RSB_NIB(11) RSB_NIB(12) RSB_NIB(13) RSB_NIB(14) RSB_NIB(15)
+#undef RSB_NIB
+  }
+  return t;
+}
+
+// d ^= c * s with c's Karatsuba factors packed in kf (k0 | k1 << 8 | k2 << 16).
+__device__ __forceinline__ void mul16_acc_rt(Reg16 &d, const Reg16 &s, uint32_t kf) {
+  Planes8 lx, hx, sx;
+#pragma unroll
+  for (int p = 0; p < 8; p++) lx.v[p] = s[p], hx.v[p] = s[8 + p], sx.v[p] = s[p] ^ s[8 + p];
+  const Planes8 t0 = mul8_rt(lx, kf & 0xff), t1 = mul8_rt(sx, (kf >> 8) & 0xff), t2 = mul8_rt(hx, kf >> 16);
+#pragma unroll
+  for (int b = 0; b < 8; b++) {
+    d[b] ^= t0.v[b] ^ t2.v[b];
+    d[8 + b] ^= t0.v[b] ^ t1.v[b];
+  }
+}
+
+__device__ __forceinline__ void bfly16_rt(Reg16 &lo, Reg16 &hi, uint32_t kf, bool inverse) {
+  if (inverse) {
+    xor16(hi, lo);
+    mul16_acc_rt(lo, hi, kf);
+  } else {
+    mul16_acc_rt(lo, hi, kf);
+    xor16(hi, lo);
+  }
+}
+
+// The factors of constant i of a table (bytes 24..26 of its entry).
+__device__ __forceinline__ uint32_t const_factors(const uint16_t *cols, uint32_t i) {
+  return *reinterpret_cast<const uint32_t *>(cols + 16 * (size_t)i + 12);
+}
+
+// fft16_pass_kernel with the constants applied through mul8_rt: no mask tables.
+template <int LV>
+__global__ void __launch_bounds__(32, 16) fft16_pass_rt_kernel(const Fft16PassArgs a) {
+  constexpr int NR = 1 << LV;
+  __shared__ __align__(16) uint4 stage[NR][4][32];  // [register][16-byte quarter][lane]
+  const uint32_t R = a.R, L = a.level, h = 1u << L, lane = threadIdx.x;
+  const uint32_t chunks = (uint32_t)((a.G + 31) / 32), tasks = a.n_stripes * chunks;
+  const uint32_t items = (R >> LV) * tasks;
+  struct Item {
+    uint32_t grp, s;
+    uint64_t g;
+  };
+  auto locate = [&](uint32_t item) {
+    Item it;
+    it.grp = item / tasks;
+    const uint32_t task = item - it.grp * tasks;
+    it.s = task / chunks;
+    it.g = (uint64_t)(task - it.s * chunks) * 32 + lane;
+    return it;
+  };
+  auto first_reg = [&](uint32_t grp) { return (grp >> L) * (h << LV) + (grp & (h - 1)); };
+  auto prefetch = [&](uint32_t item) {
+    const Item it = locate(item);
+    if (it.g < a.G) {
+      const uint32_t i0 = first_reg(it.grp);
+#pragma unroll
+      for (int q = 0; q < NR; q++) {
+        const uint32_t *p = a.src + (((uint64_t)it.s * a.src_regs + a.src_start + i0 + q * h) * a.G + it.g) * 16;
+#pragma unroll
+        for (int c = 0; c < 4; c++) cp_async16(&stage[q][c][lane], p + 4 * c);
+      }
+    }
+    cp_async_commit();
+  };
+  uint32_t item = blockIdx.x;
+  if (item < items) prefetch(item);
+  for (; item < items; item += gridDim.x) {
+    const Item it = locate(item);
+    const uint32_t blk = it.grp >> L, i0 = first_reg(it.grp);
+    uint32_t kf[LV == 2 ? 3 : 1];
+    if constexpr (LV == 2) {
+      kf[0] = const_factors(a.cols, R - (R >> L) + 2 * blk);      // level L, i0 / i0+h
+      kf[1] = const_factors(a.cols, R - (R >> L) + 2 * blk + 1);  // level L, i0+2h / i0+3h
+      kf[2] = const_factors(a.cols, R - (R >> (L + 1)) + blk);    // level L+1
+    } else {
+      kf[0] = const_factors(a.cols, R - (R >> L) + blk);
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    Reg16 r[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const uint4 v = stage[q][c][lane];
+        r[q][4 * c] = v.x, r[q][4 * c + 1] = v.y, r[q][4 * c + 2] = v.z, r[q][4 * c + 3] = v.w;
+      }
+    __syncwarp();  // the stage is read; the next item's copies may overwrite it
+    if (item + gridDim.x < items) prefetch(item + gridDim.x);
+    if (it.g >= a.G) continue;
+    if constexpr (LV == 2) {
+      if (a.inverse) {
+        bfly16_rt(r[0], r[1], kf[0], true);
+        bfly16_rt(r[2], r[3], kf[1], true);
+        bfly16_rt(r[0], r[2], kf[2], true);
+        bfly16_rt(r[1], r[3], kf[2], true);
+      } else {
+        bfly16_rt(r[0], r[2], kf[2], false);
+        bfly16_rt(r[1], r[3], kf[2], false);
+        bfly16_rt(r[0], r[1], kf[0], false);
+        bfly16_rt(r[2], r[3], kf[1], false);
+      }
+    } else {
+      bfly16_rt(r[0], r[1], kf[0], a.inverse != 0);
+    }
+    const uint64_t db = (uint64_t)it.s * a.dst_regs + a.dst_start;
+#pragma unroll
+    for (int q = 0; q < NR; q++) store_reg16(a.dst + ((db + i0 + q * h) * a.G + it.g) * 16, r[q]);
+  }
+}
+
+// Which pass kernel runs: 1 (default) the runtime-constant networks, 0 the mask tables
+// (rs_set_fft16_pass).
+inline int &fft16_pass_variant() {
+  static int v = 1;
+  return v;
+}
+
 // Launch of a pass: one warp per CTA, up to 16 per SM, persistent over the items.
 inline cudaError_t launch_fft16_pass(const Fft16PassArgs &a, int lv, cudaStream_t st) {
   const uint64_t tasks = (uint64_t)a.n_stripes * ((a.G + 31) / 32), items = ((uint64_t)a.R >> lv) * tasks;
   if (items >= (1ull << 32)) return cudaErrorInvalidValue;
   const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)sm_count() * 16));
-  if (lv == 2)
+  if (fft16_pass_variant() == 1) {
+    if (lv == 2)
+      fft16_pass_rt_kernel<2><<<grid, 32, 0, st>>>(a);
+    else
+      fft16_pass_rt_kernel<1><<<grid, 32, 0, st>>>(a);
+  } else if (lv == 2) {
     fft16_pass_kernel<2><<<grid, 32, 0, st>>>(a);
-  else
+  } else {
     fft16_pass_kernel<1><<<grid, 32, 0, st>>>(a);
+  }
   return cudaGetLastError();
 }
 

@@ -298,3 +298,20 @@ def test_decode_route_choice(gpu, O):
     shards = _erase(full, erased)
     rs.reconstruct([(s, i not in erased) for i, s in enumerate(shards)])
     assert np.array_equal(np.array(shards), full)
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+def test_both_pass_kernels_match_the_oracle(gpu, O, variant):
+    """The tower FFT pass kernel with constants through shared-memory masks (0) and
+    through compiled networks selected by the warp-uniform constant (1): the oracle's
+    bytes on shapes with one and several cosets and radix-2 tail levels."""
+    L = gpu.load()
+    old = L.rs_set_fft16_pass(variant)
+    try:
+        for k, m, length in [(8, 8, 66), (32, 96, 130), (100, 50, 64), (256, 300, 34), (1024, 64, 66)]:
+            rs = gpu.ReedSolomon16(k, m)
+            rs.set_route("fft")
+            data = _rand(k, length, k + m + variant)
+            assert np.array_equal(_encode(rs, data, m), O.encode16(k, m, data)), (k, m, length)
+    finally:
+        L.rs_set_fft16_pass(old)
