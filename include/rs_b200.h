@@ -537,6 +537,13 @@ int rs_set_fft_lanes(size_t k, int wide);
  * (parity rows per thread x output rows per CTA), 0..rs_matrix_variant_count()-1. */
 int rs_set_matrix_variant(int variant);
 int rs_matrix_variant_count(void);
+/* Tuning hook, no counterpart in the reference: the kernel of strided matrix-route
+ * calls (batched encode on the matrix route, batched and single-stripe reconstruct
+ * rows): 2 (default) the bitsliced kernel whose warp-uniform coefficients select
+ * compiled XOR networks, two output rows per network call; 1 the same, one call per
+ * coefficient; 0 the SWAR kernel. Same bytes either way. Returns the previous value,
+ * or -1 for another value. */
+int rs_set_matrix_bits(int on);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

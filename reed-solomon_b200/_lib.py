@@ -29,6 +29,7 @@ SIGNATURES = {
     "rs_set_fft_lanes": (_int, [_sz, _int]),
     "rs_set_matrix_variant": (_int, [_int]),
     "rs_set_fft16_pass": (_int, [_int]),
+    "rs_set_matrix_bits": (_int, [_int]),
     "rs_matrix_variant_count": (_int, []),
     "rs_generator_rows": (_int, [_int, _sz, _sz, _u16p, _sz]),
     "rs_decode_rows": (_int, [_int, _sz, _sz, _u8p, _u16p, _sz, _szp]),

@@ -31,6 +31,7 @@
 
 #include <cstdint>
 
+#include "kernels_bits.cuh"
 #include "kernels_fft.cuh"
 
 namespace rsb {
@@ -261,51 +262,6 @@ __global__ void __launch_bounds__(32, 16) fft16_pass_kernel(const Fft16PassArgs 
 #pragma unroll
     for (int q = 0; q < NR; q++) store_reg16(a.dst + ((db + i0 + q * h) * a.G + it.g) * 16, r[q]);
   }
-}
-
-// ---- runtime constants through compile-time networks ----
-// A butterfly constant is known only at run time, but it is the same for every lane of
-// the warp, so each of its three GF(2^8) Karatsuba factors k can select a compiled XOR
-// network instead of being applied as 64 masked XORs: k * x = (k & 15) * x + (k & 0xF0) * x,
-// and (k & 0xF0) = (k >> 4) * alpha^4 needs no reduction, so both halves are one of 16
-// compile-time constants applied to x itself (kernels_fft.cuh mul_set / mul_acc, about
-// 10 LOP3 each against 64 masked LOP3 and 16 mask loads). The two switches live in one
-// out-of-line function with its operands in registers, so the networks exist once.
-struct Planes8 {
-  uint32_t v[8];
-};
-
-template <int J>
-__device__ __forceinline__ void nib_lo(Planes8 &t, const Planes8 &x) {
-  fftc::mul_set<(uint8_t)J>(*reinterpret_cast<fftc::Reg *>(t.v), *reinterpret_cast<const fftc::Reg *>(x.v));
-}
-template <int J>
-__device__ __forceinline__ void nib_hi(Planes8 &t, const Planes8 &x) {
-  fftc::mul_acc<(uint8_t)(J << 4)>(*reinterpret_cast<fftc::Reg *>(t.v), *reinterpret_cast<const fftc::Reg *>(x.v));
-}
-
-// k * x for a warp-uniform byte k.
-__device__ __noinline__ Planes8 mul8_rt(Planes8 x, uint32_t k) {
-  Planes8 t;
-  switch (k & 15) {
-#define RSB_NIB(j)   \
-  case j:            \
-    nib_lo<j>(t, x); \
-    break;
-    RSB_NIB(0) RSB_NIB(1) RSB_NIB(2) RSB_NIB(3) RSB_NIB(4) RSB_NIB(5) RSB_NIB(6) RSB_NIB(7)
-    RSB_NIB(8) RSB_NIB(9) RSB_NIB(10) RSB_NIB(11) RSB_NIB(12) RSB_NIB(13) RSB_NIB(14) RSB_NIB(15)
-#undef RSB_NIB
-  }
-  switch ((k >> 4) & 15) {
-#define RSB_NIB(j)   \
-  case j:            \
-    nib_hi<j>(t, x); \
-    break;
-    RSB_NIB(0) RSB_NIB(1) RSB_NIB(2) RSB_NIB(3) RSB_NIB(4) RSB_NIB(5) RSB_NIB(6) RSB_NIB(7)
-    RSB_NIB(8) RSB_NIB(9) RSB_NIB(10) RSB_NIB(11) RSB_NIB(12) RSB_NIB(13) RSB_NIB(14) RSB_NIB(15)
-#undef RSB_NIB
-  }
-  return t;
 }
 
 // d ^= c * s with c's Karatsuba factors packed in kf (k0 | k1 << 8 | k2 << 16).

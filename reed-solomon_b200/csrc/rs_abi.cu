@@ -12,6 +12,7 @@
 #include "gf_host.hpp"
 #include "kernels_matrix.cuh"
 #include "kernels_fft.cuh"
+#include "kernels_bits.cuh"
 #include "kernels_plan.cuh"
 #include "codec8.hpp"
 
@@ -124,6 +125,15 @@ int launch_gf8(const ApplyArgs &a, const PtrTable *pt, bool verify, cudaStream_t
   }
   PtrTableT<false> t{};
   if (verify) return launch_gf8_t<0, false, true>(a, t, st);
+  if (matrix_bits()) {
+    g_launches++;
+    cudaError_t e = launch_gf8_bits(a, st);
+    if (e != cudaSuccess) {
+      set_cuda_error(e, "gf8_bits_kernel launch");
+      return RS_ERR_CUDA;
+    }
+    return RS_OK;
+  }
   switch (matrix_variant()) {
     case 1: return launch_gf8_t<1, false, false>(a, t, st);
     case 2: return launch_gf8_t<2, false, false>(a, t, st);
@@ -389,6 +399,13 @@ int rs_set_matrix_variant(int variant) {
 }
 
 int rs_matrix_variant_count(void) { return kMatrixVariantCount; }
+
+int rs_set_matrix_bits(int on) {
+  if (on < 0 || on > 2) return -1;
+  const int old = matrix_bits();
+  matrix_bits() = on;
+  return old;
+}
 
 int rs_set_fft_lanes(size_t k, int wide) {
   const FftShape *sh = find_fft_shape(k, k);
