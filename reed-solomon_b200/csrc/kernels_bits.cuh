@@ -5,6 +5,7 @@
 
 #include <cstdint>
 
+#include "kernels_batch.cuh"
 #include "kernels_fft.cuh"
 
 namespace rsb {
@@ -158,6 +159,60 @@ __global__ void __launch_bounds__(kBitsThreads) gf8_bits_kernel(const ApplyArgs 
   }
 }
 
+// The ragged launch's block (kernels_batch.cuh ragged_block) on the bitsliced kernel:
+// the same (row chunk, 4 KiB column tile) blocks, 128 threads of 32 columns each.
+__device__ __forceinline__ void ragged_block_bits(const RaggedItem &w, uint32_t local) {
+  static_assert(kBitsThreads * 32 == kTileBytes, "block tiles of the ragged launch");
+  const uint32_t chunk = local / w.col_tiles, tile = local % w.col_tiles;
+  const uint32_t k = w.k;
+  const uint32_t g0 = chunk * kRowChunk, g_end = min(w.rows, g0 + kRowChunk);
+  const uint64_t col = ((uint64_t)tile * kBitsThreads + threadIdx.x) * 32;
+  if (col >= w.len) return;
+  const uint64_t remain = w.len - col;
+  constexpr int OT = 8;
+  for (uint32_t g = g0; g < g_end; g += OT) {
+    const uint32_t live = min(g_end - g, (uint32_t)OT);
+    Planes8 acc[OT];
+#pragma unroll
+    for (int o = 0; o < OT; o++)
+#pragma unroll
+      for (int b = 0; b < 8; b++) acc[o].v[b] = 0;
+    for (uint32_t i = 0; i < k; i++) {
+      const uint32_t row = w.in_rows ? w.in_rows[i] : i;
+      Planes8 x = load32_fast(w.base + row * w.row_stride + col, remain);
+      bit_transpose(x.v);
+#pragma unroll
+      for (int o = 0; o < OT; o += 2) {
+        if (o < (int)live) {
+          const uint32_t c0 = __ldg(w.coeffs + (uint64_t)(g + o) * k + i);
+          const uint32_t c1 = o + 1 < (int)live ? __ldg(w.coeffs + (uint64_t)(g + o + 1) * k + i) : 0u;
+          const Planes16 t = mul8x2_rt(x, c0, c1);
+#pragma unroll
+          for (int b = 0; b < 8; b++) {
+            acc[o].v[b] ^= t.a.v[b];
+            acc[o + 1].v[b] ^= t.b.v[b];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < OT; o++) {
+      if (o < (int)live) {
+        const uint32_t row = w.out_rows ? w.out_rows[g + o] : k + g + o;
+        bit_transpose(acc[o].v);
+        store32_fast(w.base + row * w.row_stride + col, remain, acc[o]);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBitsThreads) gf8_ragged_bits_kernel(const RaggedItem *__restrict__ items,
+                                                                       uint32_t n_items) {
+  const uint32_t it = find_item(items, n_items, blockIdx.x);
+  const RaggedItem &w = items[it];
+  ragged_block_bits(w, blockIdx.x - w.block_begin);
+}
+
 // Whether launch_gf8 runs gf8_bits_kernel for strided calls (rs_set_matrix_bits): 0 no
 // (the SWAR kernel), 1 one out-of-line call per coefficient, 2 (default) one call per
 // two output rows. Measured on B200, matrix-route batched calls (RS(32,32), RS(16,16),
@@ -175,6 +230,19 @@ inline cudaError_t launch_gf8_bits_t(const ApplyArgs &a, cudaStream_t st) {
   dim3 grid((unsigned)((groups + kBitsThreads - 1) / kBitsThreads), std::min<uint32_t>(a.n_stripes, 65535),
             (a.rows + OT - 1) / OT);
   gf8_bits_kernel<OT, FORM><<<grid, kBitsThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// The ragged matrix launch (batches, the request server): the bitsliced kernel unless
+// matrix_bits() is 0. Measured on the 10,000-stripe mixed batch it runs at the SWAR
+// kernel's speed (830 GB/s batched, 148 GB/s matrix-only, both kernels). smem: the SWAR kernel's dynamic shared memory (its attribute is set
+// by the caller, outside any stream capture).
+inline cudaError_t launch_ragged(const RaggedItem *items, uint32_t n_items, uint64_t blocks, size_t smem,
+                                 cudaStream_t st) {
+  if (matrix_bits())
+    gf8_ragged_bits_kernel<<<(unsigned)blocks, kBitsThreads, 0, st>>>(items, n_items);
+  else
+    gf8_ragged_kernel<8><<<(unsigned)blocks, kThreads, smem, st>>>(items, n_items);
   return cudaGetLastError();
 }
 

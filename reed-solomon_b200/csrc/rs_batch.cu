@@ -16,6 +16,7 @@
 
 #include "codec8.hpp"
 #include "kernels_batch.cuh"
+#include "kernels_bits.cuh"
 #include "kernels_fft.cuh"
 #include "kernels_plan.cuh"
 #include "runtime.hpp"
@@ -62,9 +63,8 @@ static int batch_enqueue(rs_batch *b, cudaStream_t st) {
   for (const auto &f : b->ffts)
     RSB_TRY(launch_fft8_items(*f.shape, f.items, f.n, f.groups, st, nullptr, f.unaligned, f.cfg_wide, f.cfg_variant));
   if (b->n_ragged) {
-    gf8_ragged_kernel<8><<<(unsigned)b->ragged_blocks, kThreads, b->ragged_smem, st>>>(b->ragged, b->n_ragged);
+    RSB_CU(launch_ragged(b->ragged, b->n_ragged, b->ragged_blocks, b->ragged_smem, st));
     g_launches++;
-    RSB_CU(cudaGetLastError());
   }
   for (const auto &f : b->regens)
     RSB_TRY(launch_fft8_items(*f.shape, f.items, f.n, f.groups, st, f.masks, f.unaligned));

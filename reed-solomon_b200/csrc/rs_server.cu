@@ -40,6 +40,7 @@
 #include "fft16.hpp"
 #include "gf_host.hpp"
 #include "kernels_batch.cuh"
+#include "kernels_bits.cuh"
 #include "kernels_fft.cuh"
 #include "kernels_lagrange.cuh"
 #include "kernels_matrix.cuh"
@@ -622,11 +623,10 @@ static int enqueue_gf8(rs_server *s, Group &g, cudaStream_t st) {
     size_t smem = 8192 + (size_t)kRowChunk * max_k;
     if (smem > 48 * 1024)
       RSB_CU(cudaFuncSetAttribute(gf8_ragged_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    gf8_ragged_kernel<8><<<(unsigned)blocks, kThreads, smem, st>>>(
-        reinterpret_cast<const RaggedItem *>(gd + ragged_off), (uint32_t)ragged.size());
+    RSB_CU(launch_ragged(reinterpret_cast<const RaggedItem *>(gd + ragged_off), (uint32_t)ragged.size(), blocks,
+                         smem, st));
     g_launches++;
     g.launches++;
-    RSB_CU(cudaGetLastError());
   }
   for (auto &qp : g.reqs) RSB_TRY(stage_out(s, *qp, st));
   return RS_OK;
