@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(kBitsThreads) gf8_bits_kernel(const ApplyArgs 
 
 // The ragged launch's block (kernels_batch.cuh ragged_block) on the bitsliced kernel:
 // the same (row chunk, 4 KiB column tile) blocks, 128 threads of 32 columns each.
+template <int OT>
 __device__ __forceinline__ void ragged_block_bits(const RaggedItem &w, uint32_t local) {
   static_assert(kBitsThreads * 32 == kTileBytes, "block tiles of the ragged launch");
   const uint32_t chunk = local / w.col_tiles, tile = local % w.col_tiles;
@@ -169,7 +170,6 @@ __device__ __forceinline__ void ragged_block_bits(const RaggedItem &w, uint32_t 
   const uint64_t col = ((uint64_t)tile * kBitsThreads + threadIdx.x) * 32;
   if (col >= w.len) return;
   const uint64_t remain = w.len - col;
-  constexpr int OT = 8;
   for (uint32_t g = g0; g < g_end; g += OT) {
     const uint32_t live = min(g_end - g, (uint32_t)OT);
     Planes8 acc[OT];
@@ -206,11 +206,12 @@ __device__ __forceinline__ void ragged_block_bits(const RaggedItem &w, uint32_t 
   }
 }
 
+template <int OT>
 __global__ void __launch_bounds__(kBitsThreads) gf8_ragged_bits_kernel(const RaggedItem *__restrict__ items,
                                                                        uint32_t n_items) {
   const uint32_t it = find_item(items, n_items, blockIdx.x);
   const RaggedItem &w = items[it];
-  ragged_block_bits(w, blockIdx.x - w.block_begin);
+  ragged_block_bits<OT>(w, blockIdx.x - w.block_begin);
 }
 
 // Whether launch_gf8 runs gf8_bits_kernel for strided calls (rs_set_matrix_bits): 0 no
@@ -240,7 +241,7 @@ inline cudaError_t launch_gf8_bits_t(const ApplyArgs &a, cudaStream_t st) {
 inline cudaError_t launch_ragged(const RaggedItem *items, uint32_t n_items, uint64_t blocks, size_t smem,
                                  cudaStream_t st) {
   if (matrix_bits())
-    gf8_ragged_bits_kernel<<<(unsigned)blocks, kBitsThreads, 0, st>>>(items, n_items);
+    gf8_ragged_bits_kernel<8><<<(unsigned)blocks, kBitsThreads, 0, st>>>(items, n_items);
   else
     gf8_ragged_kernel<8><<<(unsigned)blocks, kThreads, smem, st>>>(items, n_items);
   return cudaGetLastError();
