@@ -22,8 +22,11 @@
 // A constant's table entry (16 u16) holds the column bytes k_t * 2^p of its three
 // GF(2^8) factors k0 = c_lo, k1 = c_hi + c_lo, k2 = 32 c_hi (24 bytes, 8 unused).
 //
-// Work split. The transform runs over a bitsliced scratch buffer, word
-// ((s * R + r) * G + g) * 16 + p for stripe s, register r of R, 32-symbol group g of G.
+// Work split. The transform runs over a bitsliced scratch buffer: register r of R of
+// stripe s is a block of G * 16 words at ((s * R + r) * G) * 16, holding plane p of
+// 32-symbol group g of G at word ((p / 4) * G + g) * 4 + p % 4, so the lanes of a warp
+// (consecutive groups) read and write each 16-byte quarter of their planes as one
+// contiguous 512-byte span.
 // A pass applies one or two levels. Its kernel runs one warp per CTA, persistent over
 // (butterfly group, stripe) items with one lane per 32-symbol group, so a warp's lanes
 // share the item's constants and read their masks as shared-memory broadcasts.
@@ -159,19 +162,26 @@ __device__ __forceinline__ void bfly16x2(Reg16 &lo1, Reg16 &hi1, Reg16 &lo2, Reg
   }
 }
 
-__device__ __forceinline__ void load_reg16(const uint32_t *p, Reg16 &r) {
-  const uint4 *q = reinterpret_cast<const uint4 *>(p);
+// Quarter c (planes 4c .. 4c+3) of group g in the register block at blk (G groups).
+__device__ __forceinline__ const uint32_t *quarter16(const uint32_t *blk, uint64_t G, uint64_t g, int c) {
+  return blk + ((uint64_t)c * G + g) * 4;
+}
+__device__ __forceinline__ uint32_t *quarter16(uint32_t *blk, uint64_t G, uint64_t g, int c) {
+  return blk + ((uint64_t)c * G + g) * 4;
+}
+
+__device__ __forceinline__ void load_reg16(const uint32_t *blk, uint64_t G, uint64_t g, Reg16 &r) {
 #pragma unroll
   for (int i = 0; i < 4; i++) {
-    uint4 v = q[i];
+    const uint4 v = *reinterpret_cast<const uint4 *>(quarter16(blk, G, g, i));
     r[4 * i] = v.x, r[4 * i + 1] = v.y, r[4 * i + 2] = v.z, r[4 * i + 3] = v.w;
   }
 }
 
-__device__ __forceinline__ void store_reg16(uint32_t *p, const Reg16 &r) {
-  uint4 *q = reinterpret_cast<uint4 *>(p);
+__device__ __forceinline__ void store_reg16(uint32_t *blk, uint64_t G, uint64_t g, const Reg16 &r) {
 #pragma unroll
-  for (int i = 0; i < 4; i++) q[i] = make_uint4(r[4 * i], r[4 * i + 1], r[4 * i + 2], r[4 * i + 3]);
+  for (int i = 0; i < 4; i++)
+    *reinterpret_cast<uint4 *>(quarter16(blk, G, g, i)) = make_uint4(r[4 * i], r[4 * i + 1], r[4 * i + 2], r[4 * i + 3]);
 }
 
 // LV = 1: registers {i0, i0+h} at level L (h = 2^L). LV = 2: {i0, i0+h, i0+2h, i0+3h},
@@ -209,9 +219,9 @@ __global__ void __launch_bounds__(32, 16) fft16_pass_kernel(const Fft16PassArgs 
       const uint32_t i0 = first_reg(it.grp);
 #pragma unroll
       for (int q = 0; q < NR; q++) {
-        const uint32_t *p = a.src + (((uint64_t)it.s * a.src_regs + a.src_start + i0 + q * h) * a.G + it.g) * 16;
+        const uint32_t *p = a.src + ((uint64_t)it.s * a.src_regs + a.src_start + i0 + q * h) * a.G * 16;
 #pragma unroll
-        for (int c = 0; c < 4; c++) cp_async16(&stage[q][c][lane], p + 4 * c);
+        for (int c = 0; c < 4; c++) cp_async16(&stage[q][c][lane], quarter16(p, a.G, it.g, c));
       }
     }
     cp_async_commit();
@@ -260,7 +270,7 @@ __global__ void __launch_bounds__(32, 16) fft16_pass_kernel(const Fft16PassArgs 
     }
     const uint64_t db = (uint64_t)it.s * a.dst_regs + a.dst_start;
 #pragma unroll
-    for (int q = 0; q < NR; q++) store_reg16(a.dst + ((db + i0 + q * h) * a.G + it.g) * 16, r[q]);
+    for (int q = 0; q < NR; q++) store_reg16(a.dst + (db + i0 + q * h) * a.G * 16, a.G, it.g, r[q]);
   }
 }
 
@@ -319,9 +329,9 @@ __global__ void __launch_bounds__(32, 16) fft16_pass_rt_kernel(const Fft16PassAr
       const uint32_t i0 = first_reg(it.grp);
 #pragma unroll
       for (int q = 0; q < NR; q++) {
-        const uint32_t *p = a.src + (((uint64_t)it.s * a.src_regs + a.src_start + i0 + q * h) * a.G + it.g) * 16;
+        const uint32_t *p = a.src + ((uint64_t)it.s * a.src_regs + a.src_start + i0 + q * h) * a.G * 16;
 #pragma unroll
-        for (int c = 0; c < 4; c++) cp_async16(&stage[q][c][lane], p + 4 * c);
+        for (int c = 0; c < 4; c++) cp_async16(&stage[q][c][lane], quarter16(p, a.G, it.g, c));
       }
     }
     cp_async_commit();
@@ -369,7 +379,7 @@ __global__ void __launch_bounds__(32, 16) fft16_pass_rt_kernel(const Fft16PassAr
     }
     const uint64_t db = (uint64_t)it.s * a.dst_regs + a.dst_start;
 #pragma unroll
-    for (int q = 0; q < NR; q++) store_reg16(a.dst + ((db + i0 + q * h) * a.G + it.g) * 16, r[q]);
+    for (int q = 0; q < NR; q++) store_reg16(a.dst + (db + i0 + q * h) * a.G * 16, a.G, it.g, r[q]);
   }
 }
 
@@ -417,11 +427,10 @@ __global__ void __launch_bounds__(kFft16Threads)
     load32(row + N + col, remain, hi);
     bit_transpose(lo);
     bit_transpose(hi);
-    uint4 *q = reinterpret_cast<uint4 *>(dst + ((s * R + r) * G + g) * 16);
-    q[0] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-    q[1] = make_uint4(lo[4], lo[5], lo[6], lo[7]);
-    q[2] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-    q[3] = make_uint4(hi[4], hi[5], hi[6], hi[7]);
+    Reg16 x;
+#pragma unroll
+    for (int i = 0; i < 8; i++) x[i] = lo[i], x[8 + i] = hi[i];
+    store_reg16(dst + (s * R + r) * G * 16, G, g, x);
   }
 }
 
@@ -437,10 +446,11 @@ __global__ void __launch_bounds__(kFft16Threads)
        t += (uint64_t)gridDim.x * kFft16Threads) {
     const uint64_t g = t % G, sr = t / G;
     const uint64_t r = sr % rows, s = sr / rows;
-    const uint4 *q = reinterpret_cast<const uint4 *>(src + ((s * R + r) * G + g) * 16);
-    uint4 a = q[0], b = q[1], c = q[2], d = q[3];
-    uint32_t lo[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-    uint32_t hi[8] = {c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w};
+    Reg16 x;
+    load_reg16(src + (s * R + r) * G * 16, G, g, x);
+    uint32_t lo[8], hi[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) lo[i] = x[i], hi[i] = x[8 + i];
     bit_transpose(lo);
     bit_transpose(hi);
     uint8_t *row = out_ptrs ? out_ptrs[r] : out_base + s * out_stripe + r * out_row;
@@ -466,14 +476,14 @@ __global__ void __launch_bounds__(kFft16Threads)
     const uint64_t g = t % G, si = t / G;
     const uint64_t i = si % count, s = si / count;
     Reg16 x, y;
-    load_reg16(src + ((s * src_regs + src_start + i) * G + g) * 16, x);
-    uint32_t *d = dst + ((s * dst_regs + dst_start + i) * G + g) * 16;
-    load_reg16(d, y);
+    load_reg16(src + (s * src_regs + src_start + i) * G * 16, G, g, x);
+    uint32_t *d = dst + (s * dst_regs + dst_start + i) * G * 16;
+    load_reg16(d, G, g, y);
     if (cols)
       mul16_acc(y, x, mk);
     else
       xor16(y, x);
-    store_reg16(d, y);
+    store_reg16(d, G, g, y);
   }
 }
 
@@ -526,7 +536,7 @@ __global__ void __launch_bounds__(kFft16Threads)
 #pragma unroll
       for (int i = 0; i < 16; i++) y[i] = 0;
     }
-    store_reg16(dst + ((uint64_t)r * G + g) * 16, y);
+    store_reg16(dst + (uint64_t)r * G * 16, G, g, y);
   }
 }
 
@@ -549,10 +559,10 @@ __global__ void __launch_bounds__(kFft16Threads)
     for (uint32_t t = 0; t < lg; t++) {
       if ((j >> t) & 1) continue;
       Reg16 x;
-      load_reg16(src + ((uint64_t)(j + (1u << t)) * G + g) * 16, x);
+      load_reg16(src + (uint64_t)(j + (1u << t)) * G * 16, G, g, x);
       mul16_acc(acc, x, mk[t]);
     }
-    store_reg16(dst + ((uint64_t)j * G + g) * 16, acc);
+    store_reg16(dst + (uint64_t)j * G * 16, G, g, acc);
   }
 }
 
@@ -568,7 +578,7 @@ __global__ void __launch_bounds__(kFft16Threads)
   uint8_t *row = ptrs[r];
   for (uint64_t g = threadIdx.x; g < G; g += blockDim.x) {
     Reg16 x, y;
-    load_reg16(src + ((uint64_t)r * G + g) * 16, x);
+    load_reg16(src + (uint64_t)r * G * 16, G, g, x);
     mul16_set(y, x, mk);
     uint32_t lo[8], hi[8];
 #pragma unroll
