@@ -539,10 +539,13 @@ int rs_set_matrix_variant(int variant);
 int rs_matrix_variant_count(void);
 /* Tuning hook, no counterpart in the reference: the kernel of strided matrix-route
  * calls (batched encode on the matrix route, batched and single-stripe reconstruct
- * rows): 2 (default) the bitsliced kernel whose warp-uniform coefficients select
- * compiled XOR networks, two output rows per network call; 1 the same, one call per
- * coefficient; 0 the SWAR kernel. Same bytes either way. Returns the previous value,
- * or -1 for another value. */
+ * rows) and of the ragged launches of batches and the request server: 3 (default) the
+ * lookup kernel (per input row, the XORs of every subset of each nibble's bit planes in
+ * shared memory; a coefficient is 16 lookups), 8- or 16-row output tiles by call size;
+ * 4 the same with 8-row tiles only; 2 the bitsliced kernel whose warp-uniform
+ * coefficients select compiled XOR networks, two output rows per network call; 1 the
+ * same, one call per coefficient; 0 the SWAR kernel. Same bytes either way. Returns the
+ * previous value, or -1 for another value. */
 int rs_set_matrix_bits(int on);
 
 #if defined(__GNUC__)

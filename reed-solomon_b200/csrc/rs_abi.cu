@@ -401,7 +401,7 @@ int rs_set_matrix_variant(int variant) {
 int rs_matrix_variant_count(void) { return kMatrixVariantCount; }
 
 int rs_set_matrix_bits(int on) {
-  if (on < 0 || on > 2) return -1;
+  if (on < 0 || on > 4) return -1;
   const int old = matrix_bits();
   matrix_bits() = on;
   return old;

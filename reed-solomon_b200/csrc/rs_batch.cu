@@ -45,7 +45,8 @@ struct rs_batch {
   std::vector<FftLaunch> regens;  // missing parity of reconstructs, after the data rows
   const RaggedItem *ragged = nullptr;
   uint32_t n_ragged = 0;
-  uint64_t ragged_blocks = 0;
+  uint64_t ragged_blocks[2] = {0, 0};
+  uint32_t n_ragged0 = 0;  // items in the first launch (ragged_split)
   size_t ragged_smem = 0;
   size_t launches = 0, fft_items = 0, matrix_items = 0;
   uint64_t bytes = 0;
@@ -63,8 +64,8 @@ static int batch_enqueue(rs_batch *b, cudaStream_t st) {
   for (const auto &f : b->ffts)
     RSB_TRY(launch_fft8_items(*f.shape, f.items, f.n, f.groups, st, nullptr, f.unaligned, f.cfg_wide, f.cfg_variant));
   if (b->n_ragged) {
-    RSB_CU(launch_ragged(b->ragged, b->n_ragged, b->ragged_blocks, b->ragged_smem, st));
-    g_launches++;
+    RSB_CU(launch_ragged(b->ragged, b->n_ragged0, b->n_ragged, b->ragged_blocks, b->ragged_smem, st));
+    g_launches += ragged_launches(b->ragged_blocks);
   }
   for (const auto &f : b->regens)
     RSB_TRY(launch_fft8_items(*f.shape, f.items, f.n, f.groups, st, f.masks, f.unaligned));
@@ -471,6 +472,8 @@ static int batch_create(const rs_batch_item *items, size_t n_items, int flags, c
     r.in_rows = reinterpret_cast<const uint16_t *>(base + pt.surv_off);
     r.out_rows = reinterpret_cast<const uint16_t *>(base + pt.targ_off);
   }
+  uint64_t ragged_blocks[2];
+  const uint32_t n_ragged0 = ragged_split(ragged, ragged_blocks);
   if (!ragged.empty()) memcpy(ar.host.data() + ragged_off, ragged.data(), ragged.size() * sizeof(RaggedItem));
   RSB_CU(cudaMemcpyAsync(base, ar.host.data(), ar.host.size(), cudaMemcpyHostToDevice, b->stream));
 
@@ -513,12 +516,14 @@ static int batch_create(const rs_batch_item *items, size_t n_items, int flags, c
                          reinterpret_cast<const uint32_t *>(base + f.mask_off), f.unaligned});
   b->ragged = reinterpret_cast<const RaggedItem *>(base + ragged_off);
   b->n_ragged = (uint32_t)ragged.size();
-  b->ragged_blocks = blocks;
+  b->ragged_blocks[0] = ragged_blocks[0];
+  b->ragged_blocks[1] = ragged_blocks[1];
+  b->n_ragged0 = n_ragged0;
   b->ragged_smem = 8192 + (size_t)kRowChunk * max_k;
   if (b->ragged_smem > 48 * 1024)
     RSB_CU(cudaFuncSetAttribute(gf8_ragged_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)b->ragged_smem));
-  b->launches = b->ffts.size() + b->regens.size() + (b->n_ragged ? 1 : 0);
+  b->launches = b->ffts.size() + b->regens.size() + (b->n_ragged ? ragged_launches(b->ragged_blocks) : 0);
 
   if (!(flags & RS_BATCH_NO_GRAPH) && b->launches) {
     uint64_t before = g_launches.load();

@@ -604,6 +604,8 @@ static int enqueue_gf8(rs_server *s, Group &g, cudaStream_t st) {
     off = up256(off + bytes);
   }
   size_t ragged_off = off;
+  uint64_t ragged_blocks[2];
+  const uint32_t n_ragged0 = ragged_split(ragged, ragged_blocks);
   memcpy(gh + off, ragged.data(), ragged.size() * sizeof(RaggedItem));
   off += ragged.size() * sizeof(RaggedItem);
   if (off) RSB_CU(cudaMemcpyAsync(gd, gh, off, cudaMemcpyHostToDevice, st));
@@ -623,10 +625,10 @@ static int enqueue_gf8(rs_server *s, Group &g, cudaStream_t st) {
     size_t smem = 8192 + (size_t)kRowChunk * max_k;
     if (smem > 48 * 1024)
       RSB_CU(cudaFuncSetAttribute(gf8_ragged_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    RSB_CU(launch_ragged(reinterpret_cast<const RaggedItem *>(gd + ragged_off), (uint32_t)ragged.size(), blocks,
-                         smem, st));
-    g_launches++;
-    g.launches++;
+    RSB_CU(launch_ragged(reinterpret_cast<const RaggedItem *>(gd + ragged_off), n_ragged0, (uint32_t)ragged.size(),
+                         ragged_blocks, smem, st));
+    g_launches += ragged_launches(ragged_blocks);
+    g.launches += ragged_launches(ragged_blocks);
   }
   for (auto &qp : g.reqs) RSB_TRY(stage_out(s, *qp, st));
   return RS_OK;

@@ -9,7 +9,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4])
 def test_matrix_kernels_match_the_oracle(gpu, O, mode):
     import torch
 
@@ -41,7 +41,7 @@ def test_matrix_kernels_match_the_oracle(gpu, O, mode):
         L.rs_set_matrix_bits(old)
 
 
-@pytest.mark.parametrize("mode", [0, 2])
+@pytest.mark.parametrize("mode", [0, 2, 3, 4])
 def test_ragged_batches_match_the_oracle(gpu, O, mode):
     """Mixed batches put matrix-route encodes and every reconstruct's rows on one ragged
     launch: under the SWAR (0) and the bitsliced (2) ragged kernels the stripes match the
