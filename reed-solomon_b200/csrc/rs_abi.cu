@@ -168,11 +168,15 @@ bool use_fft8(const rs8_codec *c, size_t len) {
 // missing_parity * k matrix coefficients per column (2 LOP3 per byte each, ~11 Tops/s):
 // it pays from missing_parity * k ~ 1.6 (k+m) at 3.5 TB/s. Measured on B200: RS(32,32)
 // with 8 missing parity rows +17% at 1 MiB shards, (64,64) with 16 +51%, (10,4) with 1
-// -15%. The factors below keep a margin.
+// -15%. The factors below keep a margin. With the lookup matrix kernel (twice the
+// coefficient rate of the kernels these figures came from) the generator shapes lose
+// 5-25% to the matrix route at the old factor (batches of 1..m erasures, 4 KiB - 1 MiB
+// shards), while (K,K) FFT shapes still gain 10-20% from 64 KiB; the generator shapes
+// take a higher bar.
 bool regen_parity_pays(const Gen8 &g, size_t missing_parity, int route) {
   if (!g.fft || missing_parity == 0 || route == 1) return false;
   if (route == 2) return true;
-  const size_t factor = g.k >= 128 ? 4 : g.k >= 64 ? 3 : 2;
+  const size_t factor = g.fft->gen ? 4 : g.k >= 128 ? 4 : g.k >= 64 ? 3 : 2;
   return missing_parity * g.k >= factor * (g.k + g.m);
 }
 

@@ -29,6 +29,7 @@
 #include "codec8.hpp"
 #include "gf_host.hpp"
 #include "kernels_batch.cuh"
+#include "kernels_bits.cuh"
 #include "runtime.hpp"
 
 namespace rsb {
@@ -71,15 +72,14 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Dynamic shared memory: the 8 KiB constant table and kRowChunk x 256 coefficients.
-__global__ void __launch_bounds__(kThreads)
+// A unit's blocks run on the lookup kernel's ragged block (kernels_bits.cuh), with the
+// 8-row output tile for units of at most 8 output rows.
+__global__ void __launch_bounds__(kLutThreads)
     gf8_queue_kernel(const QueueUnit *units, const QueueCtl *ctl, QueueDev *dev, unsigned long long timeout_ns) {
-  extern __shared__ __align__(16) uint32_t smem[];
-  uint32_t *R = smem;
-  uint8_t *C = reinterpret_cast<uint8_t *>(smem + 2048);
+  __shared__ __align__(16) LutShared sh;
   __shared__ QueueUnit s_unit;
   __shared__ int s_state;  // 0 run s_unit, 1 stop
-  fill_rtab(R);
+  lut_init(sh);
   for (;;) {
     if (threadIdx.x == 0) {
       const unsigned long long u = atomicAdd(&dev->next, 1ull);
@@ -108,7 +108,10 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncthreads();
     if (s_state) return;
-    for (uint32_t b = s_unit.b0; b < s_unit.b1; b++) ragged_block<8>(s_unit.item, b, R, C);
+    if (s_unit.item.rows <= 8)
+      for (uint32_t b = s_unit.b0; b < s_unit.b1; b++) ragged_block_lut<8>(s_unit.item, b, sh);
+    else
+      for (uint32_t b = s_unit.b0; b < s_unit.b1; b++) ragged_block_lut<16>(s_unit.item, b, sh);
     __syncthreads();  // every thread is done with s_unit before thread 0 claims the next
     if (threadIdx.x == 0) {
       __threadfence();
@@ -153,15 +156,14 @@ struct rs_queue {
 
 namespace rsb {
 
-// Two CTAs per SM (fewer if they do not fit): enough to keep the matrix work's loads in
-// flight, while idle CTAs stay few, each polling host memory from one thread.
+// Up to three 128-thread CTAs per SM (as many as fit): enough to keep the matrix work's
+// loads in flight, while idle CTAs stay few, each polling host memory from one thread.
 static int queue_blocks() {
   int per_sm = 0;
-  const int smem = 8192 + (int)kRowChunk * 256;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gf8_queue_kernel, kThreads, smem) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gf8_queue_kernel, kLutThreads, 0) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
-  return sm_count() * std::min(per_sm, 2);
+  return sm_count() * std::min(per_sm, 3);
 }
 
 }  // namespace rsb
@@ -187,12 +189,10 @@ int rs_queue_create(size_t max_units, size_t arena_bytes, uint64_t timeout_ns, r
   RSB_TRY(q->arena.ensure(arena_bytes ? arena_bytes : (64u << 20)));
   RSB_CU(cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking));
   RSB_CU(cudaStreamCreateWithFlags(&q->aux, cudaStreamNonBlocking));
-  const int smem = 8192 + (int)kRowChunk * 256;
-  RSB_CU(cudaFuncSetAttribute(gf8_queue_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   // The persistent launch, captured once; each session replays the graph.
   const int blocks = queue_blocks();
   RSB_CU(cudaStreamBeginCapture(q->stream, cudaStreamCaptureModeThreadLocal));
-  gf8_queue_kernel<<<blocks, kThreads, smem, q->stream>>>(q->units_d, q->ctl_d, q->dev,
+  gf8_queue_kernel<<<blocks, kLutThreads, 0, q->stream>>>(q->units_d, q->ctl_d, q->dev,
                                                                           q->timeout_ns);
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamEndCapture(q->stream, &graph);
