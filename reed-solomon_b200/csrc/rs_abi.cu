@@ -908,71 +908,79 @@ int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, s
   // on B200 (RS(32,32), 1..m erasures per stripe, both forms timed in one process):
   // +10% at 4 KiB shards, +21% at 16 KiB, +28% at 64 KiB.
   const bool split = !data_only && use_fft8(c, row_len);
-  // Host side: per-stripe survivors and targets.
-  std::vector<uint16_t> surv(n_stripes * k), targ(n_stripes * g.m), ntarg(n_stripes);
-  std::vector<int> status(n_stripes, 0);
-  std::vector<FftItem> items;       // split: stripes with missing parity
-  std::vector<uint32_t> masks;      // split: 4 words of missing parity rows per item
+  const int route = c->route.load();
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  // Device layout: one uploaded header (survivors | targets, m per stripe | target
+  // counts | parity items | parity masks), then the decode rows and plan statuses the
+  // plan kernel writes. The header is filled in pinned host memory as the stripes are
+  // scanned and goes up in one copy.
+  const size_t b_surv = n_stripes * k * 2, b_targ = n_stripes * g.m * 2, b_nt = n_stripes * 2;
+  const size_t o_targ = al(b_surv), o_nt = o_targ + al(b_targ), o_items = o_nt + al(b_nt);
+  const size_t max_header = o_items + al(n_stripes * sizeof(FftItem)) + al(n_stripes * 4 * sizeof(uint32_t));
+  Exec &ex = *c->exec;
+  std::lock_guard<std::mutex> lock(ex.mu);
+  RSB_CU(cudaSetDevice(g.device));
+  HostStage::Buf *hb = nullptr;
+  RSB_TRY(ex.stage.acquire(max_header, hb));
+  uint8_t *h = hb->ptr;
+  uint16_t *surv = reinterpret_cast<uint16_t *>(h), *targ = reinterpret_cast<uint16_t *>(h + o_targ),
+           *ntarg = reinterpret_cast<uint16_t *>(h + o_nt);
+  FftItem *items = reinterpret_cast<FftItem *>(h + o_items);  // split: stripes with missing parity
+  std::vector<uint32_t> masks;                                 // split: 4 words of missing parity rows per item
+  size_t n_items = 0;
   uint32_t max_rows = 0;
-  std::vector<uint32_t> s_surv, s_md, s_mp;
   size_t live = 0;
+  uint16_t mp[256];
   for (size_t s = 0; s < n_stripes; s++) {
-    Presence p(n);
-    size_t cnt = 0;
-    for (size_t i = 0; i < n; i++)
-      if (present[s * n + i]) {
-        p.set(i);
-        cnt++;
+    const uint8_t *pf = present + s * n;
+    uint16_t *sv = surv + s * k, *tg = targ + s * g.m;
+    size_t ns = 0, r = 0, n_mp = 0;
+    for (size_t i = 0; i < n; i++) {
+      if (pf[i]) {
+        if (ns < k) sv[ns] = (uint16_t)i;
+        ns++;
+      } else if (i < k) {
+        tg[r++] = (uint16_t)i;
+      } else {
+        mp[n_mp++] = (uint16_t)i;
       }
+    }
     ntarg[s] = 0;
-    if (cnt == n) continue;
-    if (cnt < k) {
-      status[s] = RS_TOO_FEW_SHARDS_PRESENT;
-      for (size_t t = 0; t < k; t++) surv[s * k + t] = (uint16_t)t;
+    if (statuses) statuses[s] = RS_OK;
+    if (ns == n) continue;
+    if (ns < k) {
+      if (statuses) statuses[s] = RS_TOO_FEW_SHARDS_PRESENT;
+      for (size_t t = 0; t < k; t++) sv[t] = (uint16_t)t;
       continue;
     }
-    split_pattern(p, k, n, s_surv, s_md, s_mp);
-    for (size_t t = 0; t < k; t++) surv[s * k + t] = (uint16_t)s_surv[t];
-    size_t r = 0;
-    for (uint32_t x : s_md) targ[s * g.m + r++] = (uint16_t)x;
-    if (split && regen_parity_pays(g, s_mp.size(), c->route.load())) {
+    if (split && n_mp && regen_parity_pays(g, n_mp, route)) {
       FftItem f{};
       f.in_base = d_rows + s * stripe_stride;
       f.out_base = d_rows + s * stripe_stride + k * row_len;
       f.row_stride = row_len;
       f.len = row_len;
-      f.group_begin = items.empty() ? 0 : items.back().group_begin + (row_len + 31) / 32;
-      items.push_back(f);
+      f.group_begin = n_items ? items[n_items - 1].group_begin + (row_len + 31) / 32 : 0;
+      items[n_items++] = f;
       masks.resize(masks.size() + 4, 0u);
-      for (uint32_t x : s_mp) masks[masks.size() - 4 + (x - k) / 32] |= 1u << ((x - k) % 32);
+      for (size_t j = 0; j < n_mp; j++) masks[masks.size() - 4 + (mp[j] - k) / 32] |= 1u << ((mp[j] - k) % 32);
     } else if (!data_only) {
-      for (uint32_t x : s_mp) targ[s * g.m + r++] = (uint16_t)x;
+      for (size_t j = 0; j < n_mp; j++) tg[r++] = mp[j];
     }
     ntarg[s] = (uint16_t)r;
     max_rows = std::max<uint32_t>(max_rows, (uint32_t)r);
     live++;
   }
-  if (statuses)
-    for (size_t s = 0; s < n_stripes; s++) statuses[s] = status[s];
   if (live == 0) return RS_OK;
-  Exec &ex = *c->exec;
-  std::lock_guard<std::mutex> lock(ex.mu);
-  RSB_CU(cudaSetDevice(g.device));
-  // Device layout: surv | targ (max m per stripe) | ntarg | coeff rows | plan status |
-  // parity items | parity masks.
-  size_t b_surv = surv.size() * 2, b_targ = targ.size() * 2, b_nt = ntarg.size() * 2;
-  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-  size_t o_targ = al(b_surv), o_nt = o_targ + al(b_targ), o_rows = o_nt + al(b_nt);
-  size_t b_rows = n_stripes * (size_t)g.m * k;
-  size_t o_stat = o_rows + al(b_rows);
-  size_t o_items = o_stat + al(n_stripes * sizeof(int));
-  size_t o_masks = o_items + al(items.size() * sizeof(FftItem));
-  RSB_TRY(ex.aux.ensure(o_masks + al(masks.size() * sizeof(uint32_t))));
+  const size_t o_masks = o_items + al(n_items * sizeof(FftItem));
+  const size_t header = o_masks + masks.size() * sizeof(uint32_t);
+  if (!masks.empty()) memcpy(h + o_masks, masks.data(), masks.size() * sizeof(uint32_t));
+  const size_t o_rows = al(header), b_rows = n_stripes * (size_t)g.m * k;
+  const size_t o_stat = o_rows + al(b_rows);
+  RSB_TRY(ex.aux.ensure(o_stat + al(n_stripes * sizeof(int))));
   uint8_t *base = ex.aux.ptr;
+  RSB_CU(cudaMemcpyAsync(base, h, header, cudaMemcpyHostToDevice, st));
+  RSB_TRY(ex.stage.release(*hb, st));
   if (max_rows > 0) {
-    RSB_CU(cudaMemcpyAsync(base, surv.data(), b_surv, cudaMemcpyHostToDevice, st));
-    RSB_CU(cudaMemcpyAsync(base + o_targ, targ.data(), b_targ, cudaMemcpyHostToDevice, st));
-    RSB_CU(cudaMemcpyAsync(base + o_nt, ntarg.data(), b_nt, cudaMemcpyHostToDevice, st));
     PlanArgs pa{};
     pa.gen = g.d_rows;
     pa.k = (uint32_t)k;
@@ -1007,12 +1015,9 @@ int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, s
     a.n_stripes = (uint32_t)n_stripes;
     RSB_TRY(launch_gf8(a, nullptr, false, st));
   }
-  if (items.empty()) return RS_OK;
-  RSB_CU(cudaMemcpyAsync(base + o_items, items.data(), items.size() * sizeof(FftItem), cudaMemcpyHostToDevice, st));
-  RSB_CU(cudaMemcpyAsync(base + o_masks, masks.data(), masks.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                         st));
-  const uint64_t groups = items.back().group_begin + (row_len + 31) / 32;
-  return launch_fft8_items(*g.fft, reinterpret_cast<const FftItem *>(base + o_items), (uint32_t)items.size(), groups,
+  if (n_items == 0) return RS_OK;
+  const uint64_t groups = items[n_items - 1].group_begin + (row_len + 31) / 32;
+  return launch_fft8_items(*g.fft, reinterpret_cast<const FftItem *>(base + o_items), (uint32_t)n_items, groups,
                            st, reinterpret_cast<const uint32_t *>(base + o_masks),
                            ((reinterpret_cast<uintptr_t>(d_rows) | stripe_stride | row_len) & 15) != 0);
 }

@@ -67,6 +67,54 @@ struct DeviceBuf {
   }
 };
 
+// Pinned host staging for a call's small upload (index lists, work items), two buffers
+// used in turn: a buffer is refilled only once the copy that last read it has run, so a
+// call does not wait for the previous call's device work, and its upload is one
+// asynchronous copy from pinned memory instead of several from pageable memory.
+struct HostStage {
+  struct Buf {
+    uint8_t *ptr = nullptr;
+    size_t cap = 0;
+    cudaEvent_t ev = nullptr;
+    bool pending = false;
+  };
+  Buf b[2];
+  int next = 0;
+  // The next buffer, grown to at least `bytes` and free to be written.
+  int acquire(size_t bytes, Buf *&out) {
+    Buf &x = b[next];
+    next ^= 1;
+    if (x.pending) {
+      RSB_CU(cudaEventSynchronize(x.ev));
+      x.pending = false;
+    }
+    if (bytes > x.cap) {
+      if (x.ptr) cudaFreeHost(x.ptr);
+      x.ptr = nullptr;
+      x.cap = 0;
+      const size_t want = std::max(bytes, (size_t)1 << 20);
+      RSB_CU(cudaMallocHost(&x.ptr, want));
+      x.cap = want;
+    }
+    if (!x.ev) RSB_CU(cudaEventCreateWithFlags(&x.ev, cudaEventDisableTiming));
+    out = &x;
+    return RS_OK;
+  }
+  // After the copy that reads x has been enqueued on st.
+  int release(Buf &x, cudaStream_t st) {
+    RSB_CU(cudaEventRecord(x.ev, st));
+    x.pending = true;
+    return RS_OK;
+  }
+  ~HostStage() {
+    for (Buf &x : b) {
+      if (x.pending) cudaEventSynchronize(x.ev);
+      if (x.ptr) cudaFreeHost(x.ptr);
+      if (x.ev) cudaEventDestroy(x.ev);
+    }
+  }
+};
+
 // Serialises host-pointer calls on one codec and owns their staging memory.
 struct Exec {
   static constexpr int kPipe = 3;  // streams of the pipelined host batch path
@@ -75,6 +123,7 @@ struct Exec {
   DeviceBuf buf;
   DeviceBuf aux;
   DeviceBuf pipe_buf;
+  HostStage stage;  // uploads of the batched device calls
   cudaStream_t stream = nullptr;
   cudaStream_t pipe[kPipe] = {nullptr, nullptr, nullptr};
   ~Exec() {
