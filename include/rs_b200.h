@@ -277,7 +277,11 @@ void rs_batch_free(rs_batch_t *batch);
  * and not closed gives up, and the session ends with RS_ERR_TIMEOUT (the device stays
  * usable; units published before were run). Reconstruct units use decode rows built on
  * the host and copied to the queue's device arena (arena_bytes; 0 = 64 MiB) before they
- * are published. All work runs on the matrix route. */
+ * are published. All work runs on the matrix route. While a session runs the caller
+ * frees no device or pinned memory (rs8_free included): CUDA's frees synchronize the
+ * device and would wait for the session's kernel, which ends only at close or at the
+ * timeout. The kernel keeps two CTAs per SM, leaving room for the kernels of other
+ * calls made meanwhile. */
 typedef struct rs_queue rs_queue_t;
 int rs_queue_create(size_t max_units, size_t arena_bytes, uint64_t timeout_ns, rs_queue_t **out);
 /* Begins a session (RS_ERR_INVALID_ARGUMENT while one runs). */

@@ -501,7 +501,10 @@ class Queue:
     """Persistent work queue (rs_queue_*): start() launches one persistent kernel; push()
     hands it stripes (the Batch item tuples) while it runs; finish() closes the session
     and returns its status (0, or the Timeout code 104 when a device wait gave up);
-    wait() waits without closing. Rows must stay valid until the session ends."""
+    wait() waits without closing. Rows must stay valid until the session ends. While a
+    session runs, free no device or pinned memory (destroying a codec does): CUDA's
+    frees synchronize the device and would wait for the session's kernel, which ends
+    only at close or at its timeout. start() collects garbage first for that reason."""
 
     def __init__(self, max_units=1 << 16, arena_bytes=0, timeout_s=1.0):
         self._L = _lib.load()
@@ -511,7 +514,10 @@ class Queue:
         self._hold = []
 
     def start(self):
+        import gc
+
         self._hold = []
+        gc.collect()  # pending codec frees would otherwise wait for the session's kernel
         _check(self._L.rs_queue_start(self._h))
 
     def push(self, items):

@@ -156,14 +156,18 @@ struct rs_queue {
 
 namespace rsb {
 
-// Up to three 128-thread CTAs per SM (as many as fit): enough to keep the matrix work's
-// loads in flight, while idle CTAs stay few, each polling host memory from one thread.
+// Two 128-thread CTAs per SM (fewer if they do not fit): enough to keep the matrix
+// work's loads in flight, while idle CTAs stay few, each polling host memory from one
+// thread. The persistent launch must leave every SM room for the kernels that pushes
+// enqueue while it runs (a new erasure pattern's plan kernel): three CTAs of this kernel
+// take all of an SM's registers, and a push then waited for a plan kernel that could
+// not start until the queue gave up.
 static int queue_blocks() {
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gf8_queue_kernel, kLutThreads, 0) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
-  return sm_count() * std::min(per_sm, 3);
+  return sm_count() * std::min(per_sm, 2);
 }
 
 }  // namespace rsb

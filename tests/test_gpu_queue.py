@@ -3,12 +3,27 @@ the host pushes while it runs, and its bounded device waits. The stall test make
 failure on the host (a producer that stops pushing without closing the queue): the
 kernel's waits run out, the session ends with RS_ERR_TIMEOUT, work published before is
 done, and the device and the queue stay usable. No GPU fault is involved."""
+import gc
 import time
 
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _no_frees_during_sessions():
+    """Freeing device or pinned memory (cudaFree, cudaFreeHost) synchronizes the device,
+    so a codec that the garbage collector destroys while a session runs would hold the
+    host until the session's kernel ends at its timeout. Collect first and keep the
+    collector off for the test."""
+    gc.collect()
+    gc.disable()
+    try:
+        yield
+    finally:
+        gc.enable()
 
 SHAPES = [(32, 32), (10, 10), (7, 13), (64, 64), (20, 12), (3, 5)]
 
