@@ -274,7 +274,11 @@ int fft16_decode_run(const Fft16Decode &d, const uint16_t *d_cols, uint8_t *scra
     const uint64_t gn = std::min<uint64_t>(gc, G - g0);
     uint32_t *C = reinterpret_cast<uint32_t *>(scratch), *W = C + (uint64_t)N * gn * 16;
     const unsigned rthreads = (unsigned)std::min<uint64_t>(kFft16Threads, (gn + 31) / 32 * 32);
-    fft16_scale_load_kernel<<<N, rthreads, 0, st>>>(d_ptrs, d_cols + d.row_off * 16, d.n, Nsym, g0, gn, C);
+    const bool rt = fft16_pass_variant() == 1;
+    if (rt)
+      fft16_scale_load_kernel<true><<<N, rthreads, 0, st>>>(d_ptrs, d_cols + d.row_off * 16, d.n, Nsym, g0, gn, C);
+    else
+      fft16_scale_load_kernel<false><<<N, rthreads, 0, st>>>(d_ptrs, d_cols + d.row_off * 16, d.n, Nsym, g0, gn, C);
     g_launches++;
     RSB_CU(cudaGetLastError());
     // Transforms of N registers at beta 0: inverse on C (levels 0, 1 | 2, 3 | ..., an
@@ -298,7 +302,10 @@ int fft16_decode_run(const Fft16Decode &d, const uint16_t *d_cols, uint8_t *scra
     int L = 0;
     for (; L + 1 < lg; L += 2) RSB_TRY(pass(C, L, 2, true));
     if (L < lg) RSB_TRY(pass(C, L, 1, true));
-    fft16_derivative_kernel<<<N, rthreads, 0, st>>>(C, W, d_cols + d.kappa_off * 16, d.lg, gn);
+    if (rt)
+      fft16_derivative_kernel<true><<<N, rthreads, 0, st>>>(C, W, d_cols + d.kappa_off * 16, d.lg, gn);
+    else
+      fft16_derivative_kernel<false><<<N, rthreads, 0, st>>>(C, W, d_cols + d.kappa_off * 16, d.lg, gn);
     g_launches++;
     RSB_CU(cudaGetLastError());
     int top = lg - 1;
@@ -307,8 +314,13 @@ int fft16_decode_run(const Fft16Decode &d, const uint16_t *d_cols, uint8_t *scra
       top--;
     }
     for (int l = top - 1; l >= 0; l -= 2) RSB_TRY(pass(W, l, 2, false));
-    fft16_scale_store_kernel<<<(unsigned)std::min(n_targets, d.targets.size()), rthreads, 0, st>>>(
-        W, d_targets, d_cols + d.target_off * 16, d_ptrs, Nsym, g0, gn);
+    const unsigned nt = (unsigned)std::min(n_targets, d.targets.size());
+    if (rt)
+      fft16_scale_store_kernel<true><<<nt, rthreads, 0, st>>>(W, d_targets, d_cols + d.target_off * 16, d_ptrs, Nsym,
+                                                            g0, gn);
+    else
+      fft16_scale_store_kernel<false><<<nt, rthreads, 0, st>>>(W, d_targets, d_cols + d.target_off * 16, d_ptrs, Nsym,
+                                                             g0, gn);
     g_launches++;
     RSB_CU(cudaGetLastError());
   }
@@ -447,9 +459,13 @@ int fft16_run(const Fft16Program &p, const uint16_t *d_cols, uint8_t *scratch, s
           continue;
         }
         const uint64_t items = (uint64_t)ns * s.size * gn;
-        fft16_mulxor_kernel<<<grid_for(items), kFft16Threads, 0, st>>>(
-            buf[s.src_buf], regs_of[s.src_buf], s.src_start, buf[0], regs_of[0], s.dst_start, s.size, gn, ns,
-            s.cols == Fft16Program::kNoConst ? nullptr : d_cols + s.cols * 16);
+        const uint16_t *mc = s.cols == Fft16Program::kNoConst ? nullptr : d_cols + s.cols * 16;
+        if (fft16_pass_variant() == 1)
+          fft16_mulxor_kernel<true><<<grid_for(items), kFft16Threads, 0, st>>>(
+              buf[s.src_buf], regs_of[s.src_buf], s.src_start, buf[0], regs_of[0], s.dst_start, s.size, gn, ns, mc);
+        else
+          fft16_mulxor_kernel<false><<<grid_for(items), kFft16Threads, 0, st>>>(
+              buf[s.src_buf], regs_of[s.src_buf], s.src_start, buf[0], regs_of[0], s.dst_start, s.size, gn, ns, mc);
         g_launches++;
         RSB_CU(cudaGetLastError());
       }

@@ -463,13 +463,21 @@ __global__ void __launch_bounds__(kFft16Threads)
 // Glue of the interpolation of k points that are not a power of two (src/fft.rs:198-239):
 // dst[dst_start + i] ^= c * src[src_start + i] for i < count, per stripe; with
 // cols == nullptr the constant is 1 (plain XOR).
+// RT: the constant goes through the compiled nibble networks (mul16_acc_rt) instead of
+// shared-memory masks; it is the same for every thread of the launch.
+template <bool RT>
 __global__ void __launch_bounds__(kFft16Threads)
     fft16_mulxor_kernel(const uint32_t *src, uint32_t src_regs, uint32_t src_start, uint32_t *dst, uint32_t dst_regs,
                         uint32_t dst_start, uint32_t count, uint64_t G, uint32_t n_stripes, const uint16_t *cols) {
-  __shared__ __align__(16) uint32_t mk[kMask16];
+  __shared__ __align__(16) uint32_t mk[RT ? 1 : kMask16];
+  uint32_t kf = 0;
   if (cols) {
-    for (uint32_t t = threadIdx.x; t < kMask16; t += blockDim.x) mk[t] = mask16(cols, t);
-    __syncthreads();
+    if constexpr (RT) {
+      kf = const_factors(cols, 0);
+    } else {
+      for (uint32_t t = threadIdx.x; t < kMask16; t += blockDim.x) mk[t] = mask16(cols, t);
+      __syncthreads();
+    }
   }
   const uint64_t total = (uint64_t)n_stripes * count * G;
   for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
@@ -479,10 +487,12 @@ __global__ void __launch_bounds__(kFft16Threads)
     load_reg16(src + (s * src_regs + src_start + i) * G * 16, G, g, x);
     uint32_t *d = dst + (s * dst_regs + dst_start + i) * G * 16;
     load_reg16(d, G, g, y);
-    if (cols)
-      mul16_acc(y, x, mk);
-    else
+    if (!cols)
       xor16(y, x);
+    else if constexpr (RT)
+      mul16_acc_rt(y, x, kf);
+    else
+      mul16_acc(y, x, mk);
     store_reg16(d, G, g, y);
   }
 }
@@ -504,10 +514,11 @@ __device__ __forceinline__ void mul16_set(Reg16 &d, const Reg16 &s, const uint32
 // Register r of C (one CTA per register, N of them): the shard at point r times its
 // constant c_r (cols + 16 r), or zero where c_r = 0 (erased points and padding past
 // the last shard, whose pointer is not read). Symbol groups g0 .. g0+G-1.
+template <bool RT>
 __global__ void __launch_bounds__(kFft16Threads)
     fft16_scale_load_kernel(const uint8_t *const *ptrs, const uint16_t *cols, uint32_t n, uint64_t Nsym,
                             uint64_t g0, uint64_t G, uint32_t *dst) {
-  __shared__ __align__(16) uint32_t mk[kMask16];
+  __shared__ __align__(16) uint32_t mk[RT ? 1 : kMask16];
   __shared__ int live;
   const uint32_t r = blockIdx.x;
   const uint16_t *c = cols + 16 * (uint64_t)r;
@@ -516,7 +527,11 @@ __global__ void __launch_bounds__(kFft16Threads)
     for (int p = 0; p < 16; p++) any |= c[p];
     live = r < n && any;
   }
-  masks_from_cols(mk, c);
+  uint32_t kf = 0;
+  if constexpr (RT)
+    kf = const_factors(c, 0);
+  else
+    masks_from_cols(mk, c);
   __syncthreads();
   for (uint64_t g = threadIdx.x; g < G; g += blockDim.x) {
     Reg16 y;
@@ -531,7 +546,13 @@ __global__ void __launch_bounds__(kFft16Threads)
       Reg16 x;
 #pragma unroll
       for (int i = 0; i < 8; i++) x[i] = lo[i], x[8 + i] = hi[i];
-      mul16_set(y, x, mk);
+      if constexpr (RT) {
+#pragma unroll
+        for (int i = 0; i < 16; i++) y[i] = 0;
+        mul16_acc_rt(y, x, kf);
+      } else {
+        mul16_set(y, x, mk);
+      }
     } else {
 #pragma unroll
       for (int i = 0; i < 16; i++) y[i] = 0;
@@ -543,15 +564,18 @@ __global__ void __launch_bounds__(kFft16Threads)
 // Formal derivative in the novel basis (one CTA per output register j < N):
 // D_j = sum over levels t with bit t of j clear of kappa_t * C_{j + 2^t}, kappa_t the
 // constant derivative of the normalised subspace polynomial of level t.
+template <bool RT>
 __global__ void __launch_bounds__(kFft16Threads)
     fft16_derivative_kernel(const uint32_t *src, uint32_t *dst, const uint16_t *kcols, uint32_t lg, uint64_t G) {
-  __shared__ __align__(16) uint32_t mk[16][kMask16];
+  __shared__ __align__(16) uint32_t mk[RT ? 1 : 16][RT ? 1 : kMask16];
   const uint32_t j = blockIdx.x;
-  for (uint32_t t = threadIdx.x; t < lg * kMask16; t += blockDim.x) {
-    const uint32_t c = t / kMask16, w = t - c * kMask16;
-    mk[c][w] = mask16(kcols + 16 * c, w);
+  if constexpr (!RT) {
+    for (uint32_t t = threadIdx.x; t < lg * kMask16; t += blockDim.x) {
+      const uint32_t c = t / kMask16, w = t - c * kMask16;
+      mk[c][w] = mask16(kcols + 16 * c, w);
+    }
+    __syncthreads();
   }
-  __syncthreads();
   for (uint64_t g = threadIdx.x; g < G; g += blockDim.x) {
     Reg16 acc;
 #pragma unroll
@@ -560,7 +584,10 @@ __global__ void __launch_bounds__(kFft16Threads)
       if ((j >> t) & 1) continue;
       Reg16 x;
       load_reg16(src + (uint64_t)(j + (1u << t)) * G * 16, G, g, x);
-      mul16_acc(acc, x, mk[t]);
+      if constexpr (RT)
+        mul16_acc_rt(acc, x, const_factors(kcols, t));
+      else
+        mul16_acc(acc, x, mk[t]);
     }
     store_reg16(dst + (uint64_t)j * G * 16, G, g, acc);
   }
@@ -568,18 +595,29 @@ __global__ void __launch_bounds__(kFft16Threads)
 
 // Rebuilt shards (one CTA per target i): point rows[i] of W times its constant
 // (tcols + 16 i), back to bytes at ptrs[rows[i]].
+template <bool RT>
 __global__ void __launch_bounds__(kFft16Threads)
     fft16_scale_store_kernel(const uint32_t *src, const uint32_t *rows, const uint16_t *tcols,
                              uint8_t *const *ptrs, uint64_t Nsym, uint64_t g0, uint64_t G) {
-  __shared__ __align__(16) uint32_t mk[kMask16];
+  __shared__ __align__(16) uint32_t mk[RT ? 1 : kMask16];
   const uint32_t i = blockIdx.x, r = rows[i];
-  masks_from_cols(mk, tcols + 16 * (uint64_t)i);
+  uint32_t kf = 0;
+  if constexpr (RT)
+    kf = const_factors(tcols, i);
+  else
+    masks_from_cols(mk, tcols + 16 * (uint64_t)i);
   __syncthreads();
   uint8_t *row = ptrs[r];
   for (uint64_t g = threadIdx.x; g < G; g += blockDim.x) {
     Reg16 x, y;
     load_reg16(src + (uint64_t)r * G * 16, G, g, x);
-    mul16_set(y, x, mk);
+    if constexpr (RT) {
+#pragma unroll
+      for (int b = 0; b < 16; b++) y[b] = 0;
+      mul16_acc_rt(y, x, kf);
+    } else {
+      mul16_set(y, x, mk);
+    }
     uint32_t lo[8], hi[8];
 #pragma unroll
     for (int b = 0; b < 8; b++) lo[b] = y[b], hi[b] = y[8 + b];

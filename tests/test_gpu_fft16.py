@@ -313,5 +313,18 @@ def test_both_pass_kernels_match_the_oracle(gpu, O, variant):
             rs.set_route("fft")
             data = _rand(k, length, k + m + variant)
             assert np.array_equal(_encode(rs, data, m), O.encode16(k, m, data)), (k, m, length)
+        # The erasure decoder's load, derivative and store kernels under the same switch.
+        rng = np.random.default_rng(40 + variant)
+        for k, m, length in [(7, 13, 66), (100, 50, 130), (300, 200, 34)]:
+            rs = gpu.ReedSolomon16(k, m)
+            rs.set_route("fft")
+            n = k + m
+            data = _rand(k, length, 3 * k + variant)
+            full = np.concatenate([data, O.encode16(k, m, data)])
+            for erased in ([0], list(range(k, n)),
+                           sorted(rng.choice(n, size=m, replace=False).tolist())):
+                shards = _erase(full, erased)
+                rs.reconstruct([(sh, i not in erased) for i, sh in enumerate(shards)])
+                assert np.array_equal(np.array(shards), full), (k, m, erased)
     finally:
         L.rs_set_fft16_pass(old)
