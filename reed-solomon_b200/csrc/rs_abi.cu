@@ -168,15 +168,17 @@ bool use_fft8(const rs8_codec *c, size_t len) {
 // missing_parity * k matrix coefficients per column (2 LOP3 per byte each, ~11 Tops/s):
 // it pays from missing_parity * k ~ 1.6 (k+m) at 3.5 TB/s. Measured on B200: RS(32,32)
 // with 8 missing parity rows +17% at 1 MiB shards, (64,64) with 16 +51%, (10,4) with 1
-// -15%. The factors below keep a margin. With the lookup matrix kernel (twice the
-// coefficient rate of the kernels these figures came from) the generator shapes lose
-// 5-25% to the matrix route at the old factor (batches of 1..m erasures, 4 KiB - 1 MiB
-// shards), while (K,K) FFT shapes still gain 10-20% from 64 KiB; the generator shapes
-// take a higher bar.
+// -15%. With the subset-table matrix kernel (twice the coefficient rate of the kernels
+// these figures came from) the bar rose; the factors below come from a sweep of 0.5-3x
+// the earlier ones on batches of 1..m erasures at 4 KiB, 64 KiB and 1 MiB (B200):
+// (128,128) best at 3x (up to 11% at 1 MiB), (64,64) at 2x, (32,32) at 1.5x, (16,16)
+// at 1x, the generator shapes from 1.5x of a factor of 4 ((20,12) at 4 KiB 22%); all
+// within a few percent of the best of the sweep, and regeneration still beats none
+// (up to 25%).
 bool regen_parity_pays(const Gen8 &g, size_t missing_parity, int route) {
   if (!g.fft || missing_parity == 0 || route == 1) return false;
   if (route == 2) return true;
-  const size_t factor = g.fft->gen ? 4 : g.k >= 128 ? 4 : g.k >= 64 ? 3 : 2;
+  const size_t factor = g.fft->gen ? 6 : g.k >= 128 ? 12 : g.k >= 64 ? 6 : g.k >= 32 ? 3 : 2;
   return missing_parity * g.k >= factor * (g.k + g.m);
 }
 
@@ -930,21 +932,21 @@ int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, s
   size_t n_items = 0;
   uint32_t max_rows = 0;
   size_t live = 0;
-  uint16_t mp[256];
+  // Per stripe, one branch-free pass sorts the shard indexes into present, missing data
+  // and missing parity (random flags made the branchy scan mispredict: 2.7x slower).
+  uint16_t ls[257], md[257], mp[257];
   for (size_t s = 0; s < n_stripes; s++) {
     const uint8_t *pf = present + s * n;
     uint16_t *sv = surv + s * k, *tg = targ + s * g.m;
     size_t ns = 0, r = 0, n_mp = 0;
     for (size_t i = 0; i < n; i++) {
-      if (pf[i]) {
-        if (ns < k) sv[ns] = (uint16_t)i;
-        ns++;
-      } else if (i < k) {
-        tg[r++] = (uint16_t)i;
-      } else {
-        mp[n_mp++] = (uint16_t)i;
-      }
+      const size_t pr = pf[i] != 0, dat = i < k;
+      ls[ns] = md[r] = mp[n_mp] = (uint16_t)i;
+      ns += pr;
+      r += (pr ^ 1) & dat;
+      n_mp += (pr ^ 1) & (dat ^ 1);
     }
+    memcpy(sv, ls, 2 * std::min(ns, k));
     ntarg[s] = 0;
     if (statuses) statuses[s] = RS_OK;
     if (ns == n) continue;
@@ -953,6 +955,7 @@ int rs8_reconstruct_batch_dev(rs8_t *c, uint8_t *d_rows, size_t stripe_stride, s
       for (size_t t = 0; t < k; t++) sv[t] = (uint16_t)t;
       continue;
     }
+    memcpy(tg, md, 2 * r);  // r <= n - ns <= m once k shards are present
     if (split && n_mp && regen_parity_pays(g, n_mp, route)) {
       FftItem f{};
       f.in_base = d_rows + s * stripe_stride;
