@@ -323,8 +323,18 @@ __global__ void __launch_bounds__(32, 16) fft16_pass_rt_kernel(const Fft16PassAr
     return it;
   };
   auto first_reg = [&](uint32_t grp) { return (grp >> L) * (h << LV) + (grp & (h - 1)); };
+  constexpr int NK = LV == 2 ? 3 : 1;
+  uint32_t kf_next[NK];  // the next item's constants, loaded with its registers
   auto prefetch = [&](uint32_t item) {
     const Item it = locate(item);
+    const uint32_t blk = it.grp >> L;
+    if constexpr (LV == 2) {
+      kf_next[0] = const_factors(a.cols, R - (R >> L) + 2 * blk);      // level L, i0 / i0+h
+      kf_next[1] = const_factors(a.cols, R - (R >> L) + 2 * blk + 1);  // level L, i0+2h / i0+3h
+      kf_next[2] = const_factors(a.cols, R - (R >> (L + 1)) + blk);    // level L+1
+    } else {
+      kf_next[0] = const_factors(a.cols, R - (R >> L) + blk);
+    }
     if (it.g < a.G) {
       const uint32_t i0 = first_reg(it.grp);
 #pragma unroll
@@ -340,15 +350,10 @@ __global__ void __launch_bounds__(32, 16) fft16_pass_rt_kernel(const Fft16PassAr
   if (item < items) prefetch(item);
   for (; item < items; item += gridDim.x) {
     const Item it = locate(item);
-    const uint32_t blk = it.grp >> L, i0 = first_reg(it.grp);
-    uint32_t kf[LV == 2 ? 3 : 1];
-    if constexpr (LV == 2) {
-      kf[0] = const_factors(a.cols, R - (R >> L) + 2 * blk);      // level L, i0 / i0+h
-      kf[1] = const_factors(a.cols, R - (R >> L) + 2 * blk + 1);  // level L, i0+2h / i0+3h
-      kf[2] = const_factors(a.cols, R - (R >> (L + 1)) + blk);    // level L+1
-    } else {
-      kf[0] = const_factors(a.cols, R - (R >> L) + blk);
-    }
+    const uint32_t i0 = first_reg(it.grp);
+    uint32_t kf[NK];
+#pragma unroll
+    for (int c = 0; c < NK; c++) kf[c] = kf_next[c];
     cp_async_wait_all();
     __syncwarp();
     Reg16 r[NR];
