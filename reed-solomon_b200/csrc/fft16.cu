@@ -274,7 +274,7 @@ int fft16_decode_run(const Fft16Decode &d, const uint16_t *d_cols, uint8_t *scra
     const uint64_t gn = std::min<uint64_t>(gc, G - g0);
     uint32_t *C = reinterpret_cast<uint32_t *>(scratch), *W = C + (uint64_t)N * gn * 16;
     const unsigned rthreads = (unsigned)std::min<uint64_t>(kFft16Threads, (gn + 31) / 32 * 32);
-    const bool rt = fft16_pass_variant() == 1;
+    const bool rt = fft16_rt();
     if (rt)
       fft16_scale_load_kernel<true><<<N, rthreads, 0, st>>>(d_ptrs, d_cols + d.row_off * 16, d.n, Nsym, g0, gn, C);
     else
@@ -299,21 +299,17 @@ int fft16_decode_run(const Fft16Decode &d, const uint16_t *d_cols, uint8_t *scra
       return RS_OK;
     };
     const int lg = (int)d.lg;
-    int L = 0;
-    for (; L + 1 < lg; L += 2) RSB_TRY(pass(C, L, 2, true));
-    if (L < lg) RSB_TRY(pass(C, L, 1, true));
+    int plan[40][2];
+    const int np_inv = fft16_passes(lg, true, plan);
+    for (int i = 0; i < np_inv; i++) RSB_TRY(pass(C, plan[i][0], plan[i][1], true));
     if (rt)
       fft16_derivative_kernel<true><<<N, rthreads, 0, st>>>(C, W, d_cols + d.kappa_off * 16, d.lg, gn);
     else
       fft16_derivative_kernel<false><<<N, rthreads, 0, st>>>(C, W, d_cols + d.kappa_off * 16, d.lg, gn);
     g_launches++;
     RSB_CU(cudaGetLastError());
-    int top = lg - 1;
-    if (lg % 2 == 1) {
-      RSB_TRY(pass(W, top, 1, false));
-      top--;
-    }
-    for (int l = top - 1; l >= 0; l -= 2) RSB_TRY(pass(W, l, 2, false));
+    const int np_fwd = fft16_passes(lg, false, plan);
+    for (int i = 0; i < np_fwd; i++) RSB_TRY(pass(W, plan[i][0], plan[i][1], false));
     const unsigned nt = (unsigned)std::min(n_targets, d.targets.size());
     if (rt)
       fft16_scale_store_kernel<true><<<nt, rthreads, 0, st>>>(W, d_targets, d_cols + d.target_off * 16, d_ptrs, Nsym,
@@ -337,9 +333,9 @@ bool fft16_preferred(const Fft16Program &p) {
 
 static double fft16_time_us(const Fft16Program &p, size_t len, size_t n_stripes) {
   auto passes = [](uint64_t size) {
-    int lg = 0;
+    int lg = 0, plan[40][2];
     while ((1ull << lg) < size) lg++;
-    return (uint64_t)(lg + 1) / 2;
+    return (uint64_t)fft16_passes(lg, true, plan);
   };
   uint64_t launches = 1 + (p.k < p.t ? 1 : 0);  // load (+ zeroing)
   for (const Fft16Step &s : p.interp) launches += s.kind == Fft16Step::kTransform ? passes(s.size) : 1;
@@ -423,24 +419,11 @@ int fft16_run(const Fft16Program &p, const uint16_t *d_cols, uint8_t *scratch, s
           src_regs = regs_of[s.dst_buf];
           src_start = s.dst_start;
         };
-        if (s.inverse) {
-          int L = 0;
-          for (; L + 1 < lg; L += 2) {
-            RSB_TRY(pass(s, src, src_regs, src_start, L, 2));
-            advance();
-          }
-          if (L < lg) RSB_TRY(pass(s, src, src_regs, src_start, L, 1));
-        } else {
-          int top = lg - 1;
-          if (lg % 2 == 1) {
-            RSB_TRY(pass(s, src, src_regs, src_start, top, 1));
-            advance();
-            top--;
-          }
-          for (int l = top - 1; l >= 0; l -= 2) {
-            RSB_TRY(pass(s, src, src_regs, src_start, l, 2));
-            advance();
-          }
+        int plan[40][2];
+        const int np = fft16_passes(lg, s.inverse != 0, plan);
+        for (int i = 0; i < np; i++) {
+          RSB_TRY(pass(s, src, src_regs, src_start, plan[i][0], plan[i][1]));
+          advance();
         }
         return RS_OK;
       };
@@ -460,7 +443,7 @@ int fft16_run(const Fft16Program &p, const uint16_t *d_cols, uint8_t *scratch, s
         }
         const uint64_t items = (uint64_t)ns * s.size * gn;
         const uint16_t *mc = s.cols == Fft16Program::kNoConst ? nullptr : d_cols + s.cols * 16;
-        if (fft16_pass_variant() == 1)
+        if (fft16_rt())
           fft16_mulxor_kernel<true><<<grid_for(items), kFft16Threads, 0, st>>>(
               buf[s.src_buf], regs_of[s.src_buf], s.src_start, buf[0], regs_of[0], s.dst_start, s.size, gn, ns, mc);
         else
@@ -493,7 +476,7 @@ int fft16_run(const Fft16Program &p, const uint16_t *d_cols, uint8_t *scratch, s
 }  // namespace rsb
 
 extern "C" int rs_set_fft16_pass(int variant) {
-  if (variant < 0 || variant > 1) return -1;
+  if (variant < 0 || variant > 2) return -1;
   const int old = rsb::fft16_pass_variant();
   rsb::fft16_pass_variant() = variant;
   return old;

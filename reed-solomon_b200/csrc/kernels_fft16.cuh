@@ -388,19 +388,151 @@ __global__ void __launch_bounds__(32, 16) fft16_pass_rt_kernel(const Fft16PassAr
   }
 }
 
-// Which pass kernel runs: 1 (default) the runtime-constant networks, 0 the mask tables
-// (rs_set_fft16_pass).
+// Radix-16 pass with the runtime-constant networks: levels L .. L+3 of one item's 16
+// registers {i0 + q h : q = 0..15}, four warps per CTA. The item's registers are staged
+// in shared memory (32 KiB); warp w runs two levels on one grouping of four registers,
+// the CTA exchanges through shared memory, and warp w runs the other two levels on the
+// other grouping and stores. Inverse: levels L, L+1 on registers 4w .. 4w+3, then L+2,
+// L+3 on w, w+4, w+8, w+12; forward: the mirror image. The constant of level L+l for the
+// block at register i0 + q h is entry R - (R >> (L+l)) + ((grp >> L) << (3-l)) + (q >> (l+1)),
+// as in the radix-4 kernels. Each item reads and writes the scratch once for four levels
+// instead of two.
+__global__ void __launch_bounds__(128, 4) fft16_pass16_kernel(const Fft16PassArgs a) {
+  __shared__ __align__(16) uint4 stage[16][4][32];  // [register][16-byte quarter][lane]
+  const uint32_t R = a.R, L = a.level, h = 1u << L;
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t chunks = (uint32_t)((a.G + 31) / 32), tasks = a.n_stripes * chunks;
+  const uint32_t items = (R >> 4) * tasks;
+  auto cidx = [&](uint32_t l, uint32_t gb, uint32_t q) {
+    return R - (R >> (L + l)) + (gb << (3 - l)) + (q >> (l + 1));
+  };
+  for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
+    const uint32_t grp = item / tasks, task = item - grp * tasks;
+    const uint32_t s = task / chunks;
+    const uint64_t gbase = (uint64_t)(task - s * chunks) * 32;
+    const uint32_t gb = grp >> L, i0 = gb * (h << 4) + (grp & (h - 1));
+    const uint64_t rstride = (uint64_t)h * a.G * 16;  // words between the item's registers
+    const uint32_t *sbase = a.src + ((uint64_t)s * a.src_regs + a.src_start + i0) * a.G * 16;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      const uint32_t idx = threadIdx.x + 128u * i;
+      const uint32_t ln = idx & 31u, c = (idx >> 5) & 3u, q = idx >> 7;
+      const uint64_t g = gbase + ln;
+      if (g < a.G) cp_async16(&stage[q][c][ln], quarter16(sbase + q * rstride, a.G, g, c));
+    }
+    cp_async_commit();
+    // This warp's six constants (two levels per grouping), loaded while the copies land.
+    uint32_t ka[3], kb[3];
+    if (a.inverse) {
+      ka[0] = const_factors(a.cols, cidx(0, gb, 4 * w));
+      ka[1] = const_factors(a.cols, cidx(0, gb, 4 * w + 2));
+      ka[2] = const_factors(a.cols, cidx(1, gb, 4 * w));
+      kb[0] = const_factors(a.cols, cidx(2, gb, w));
+      kb[1] = const_factors(a.cols, cidx(2, gb, w + 8));
+      kb[2] = const_factors(a.cols, cidx(3, gb, w));
+    } else {
+      ka[0] = const_factors(a.cols, cidx(2, gb, w));
+      ka[1] = const_factors(a.cols, cidx(2, gb, w + 8));
+      ka[2] = const_factors(a.cols, cidx(3, gb, w));
+      kb[0] = const_factors(a.cols, cidx(0, gb, 4 * w));
+      kb[1] = const_factors(a.cols, cidx(0, gb, 4 * w + 2));
+      kb[2] = const_factors(a.cols, cidx(1, gb, 4 * w));
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // First grouping: inverse 4w + j, forward w + 4j.
+    const uint32_t qa = a.inverse ? 4 * w : w, sa = a.inverse ? 1 : 4;
+    const uint32_t qb = a.inverse ? w : 4 * w, sb = a.inverse ? 4 : 1;
+    Reg16 r[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const uint4 v = stage[qa + j * sa][c][lane];
+        r[j][4 * c] = v.x, r[j][4 * c + 1] = v.y, r[j][4 * c + 2] = v.z, r[j][4 * c + 3] = v.w;
+      }
+    if (a.inverse) {
+      bfly16_rt(r[0], r[1], ka[0], true);
+      bfly16_rt(r[2], r[3], ka[1], true);
+      bfly16_rt(r[0], r[2], ka[2], true);
+      bfly16_rt(r[1], r[3], ka[2], true);
+    } else {
+      bfly16_rt(r[0], r[2], ka[2], false);
+      bfly16_rt(r[1], r[3], ka[2], false);
+      bfly16_rt(r[0], r[1], ka[0], false);
+      bfly16_rt(r[2], r[3], ka[1], false);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int c = 0; c < 4; c++)
+        stage[qa + j * sa][c][lane] = make_uint4(r[j][4 * c], r[j][4 * c + 1], r[j][4 * c + 2], r[j][4 * c + 3]);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const uint4 v = stage[qb + j * sb][c][lane];
+        r[j][4 * c] = v.x, r[j][4 * c + 1] = v.y, r[j][4 * c + 2] = v.z, r[j][4 * c + 3] = v.w;
+      }
+    __syncthreads();  // the stage is free for the next item's copies
+    if (a.inverse) {
+      bfly16_rt(r[0], r[1], kb[0], true);
+      bfly16_rt(r[2], r[3], kb[1], true);
+      bfly16_rt(r[0], r[2], kb[2], true);
+      bfly16_rt(r[1], r[3], kb[2], true);
+    } else {
+      bfly16_rt(r[0], r[2], kb[2], false);
+      bfly16_rt(r[1], r[3], kb[2], false);
+      bfly16_rt(r[0], r[1], kb[0], false);
+      bfly16_rt(r[2], r[3], kb[1], false);
+    }
+    const uint64_t g = gbase + lane;
+    if (g < a.G) {
+      const uint64_t db = (uint64_t)s * a.dst_regs + a.dst_start + i0;
+#pragma unroll
+      for (int j = 0; j < 4; j++) store_reg16(a.dst + (db + (uint64_t)(qb + j * sb) * h) * a.G * 16, a.G, g, r[j]);
+    }
+  }
+}
+
+// Which pass kernels run (rs_set_fft16_pass): 2 (default) the runtime-constant networks
+// with radix-16 passes where four levels remain, then radix-4 and radix-2; 1 the same
+// networks in radix-4 passes only; 0 the mask tables. The scaling, glue and store kernels
+// take the runtime-constant networks for 1 and 2. Measured on B200 (2 KiB shards): 2
+// against 1, (1024,1024) x 64 stripes 411 -> 463 GB/s, (4096,12288) x 2 240 -> 312 GB/s.
 inline int &fft16_pass_variant() {
-  static int v = 1;
+  static int v = 2;
   return v;
+}
+inline bool fft16_rt() { return fft16_pass_variant() >= 1; }
+
+// The passes of a transform of 2^lg registers, in launch order: (lowest level, levels).
+// Inverse: levels ascending, four at a time when radix-16 passes run, then two, then an
+// odd top level alone; forward: the same passes in reverse order.
+inline int fft16_passes(int lg, bool inverse, int (*out)[2]) {
+  int n = 0, L = 0;
+  if (fft16_pass_variant() == 2)
+    for (; L + 3 < lg; L += 4) out[n][0] = L, out[n++][1] = 4;
+  for (; L + 1 < lg; L += 2) out[n][0] = L, out[n++][1] = 2;
+  if (L < lg) out[n][0] = L, out[n++][1] = 1;
+  if (!inverse)
+    for (int i = 0; i < n / 2; i++)
+      for (int j = 0; j < 2; j++) std::swap(out[i][j], out[n - 1 - i][j]);
+  return n;
 }
 
 // Launch of a pass: one warp per CTA, up to 16 per SM, persistent over the items.
 inline cudaError_t launch_fft16_pass(const Fft16PassArgs &a, int lv, cudaStream_t st) {
   const uint64_t tasks = (uint64_t)a.n_stripes * ((a.G + 31) / 32), items = ((uint64_t)a.R >> lv) * tasks;
   if (items >= (1ull << 32)) return cudaErrorInvalidValue;
+  if (lv == 4) {  // four 128-thread CTAs per SM (registers)
+    const unsigned g4 = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)sm_count() * 4));
+    fft16_pass16_kernel<<<g4, 128, 0, st>>>(a);
+    return cudaGetLastError();
+  }
   const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)sm_count() * 16));
-  if (fft16_pass_variant() == 1) {
+  if (fft16_rt()) {
     if (lv == 2)
       fft16_pass_rt_kernel<2><<<grid, 32, 0, st>>>(a);
     else

@@ -300,11 +300,12 @@ def test_decode_route_choice(gpu, O):
     assert np.array_equal(np.array(shards), full)
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 def test_both_pass_kernels_match_the_oracle(gpu, O, variant):
-    """The tower FFT pass kernel with constants through shared-memory masks (0) and
-    through compiled networks selected by the warp-uniform constant (1): the oracle's
-    bytes on shapes with one and several cosets and radix-2 tail levels."""
+    """The tower FFT pass kernel with constants through shared-memory masks (0), through
+    compiled networks selected by the warp-uniform constant (1), and the latter with
+    radix-16 passes (2: four levels per pass where four remain, then radix-4 and radix-2
+    tails): the oracle's bytes on shapes with one and several cosets."""
     L = gpu.load()
     old = L.rs_set_fft16_pass(variant)
     try:
@@ -326,5 +327,32 @@ def test_both_pass_kernels_match_the_oracle(gpu, O, variant):
                 shards = _erase(full, erased)
                 rs.reconstruct([(sh, i not in erased) for i, sh in enumerate(shards)])
                 assert np.array_equal(np.array(shards), full), (k, m, erased)
+    finally:
+        L.rs_set_fft16_pass(old)
+
+
+def test_pass_kernel_variants_agree_on_large_batches(gpu, O):
+    """Launches with several items per CTA and more items than one grid stride: pass
+    variants 0, 1 and 2 give the same bytes, and stripe 0 equals the oracle."""
+    import torch
+
+    L = gpu.load()
+    old = L.rs_set_fft16_pass(1)
+    try:
+        for k, m, S, stripes in [(256, 256, 8192, 17), (1000, 24, 4098, 5)]:
+            rs = gpu.ReedSolomon16(k, m)
+            rs.set_route("fft")
+            g = torch.Generator(device="cuda").manual_seed(k)
+            d = torch.randint(0, 256, (stripes, k, S), dtype=torch.uint8, device="cuda", generator=g)
+            outs = []
+            for variant in (1, 2, 0):
+                L.rs_set_fft16_pass(variant)
+                p = torch.full((stripes, m, S), 0xA5, dtype=torch.uint8, device="cuda")
+                rs.encode_batch_dev(d, p, S, stripes)
+                torch.cuda.synchronize()
+                outs.append(p)
+            assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2]), (k, m)
+            host = d[0].cpu().numpy()
+            assert np.array_equal(outs[1][0].cpu().numpy(), O.encode16(k, m, host)), (k, m)
     finally:
         L.rs_set_fft16_pass(old)
