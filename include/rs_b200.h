@@ -425,9 +425,10 @@ const char *rs16_encode_route_for(const rs16_t *codec, size_t len, size_t n_stri
 int rs16_set_route(rs16_t *codec, int route);
 /* Tuning hook, no counterpart in the reference: the tower FFT pass kernels, 2 (default)
  * runtime constants dispatched to compiled XOR networks, in passes of four levels
- * (radix 16, through shared memory) where four remain; 1 the same networks in passes of
- * two levels; 0 constants applied through shared-memory mask tables. All give the same
- * bytes. Returns the previous value, or -1 for another value. */
+ * (radix 16, through shared memory), of five for one pass when the level count is odd,
+ * then of two; 1 the same networks in passes of two levels; 0 constants applied through
+ * shared-memory mask tables. All give the same bytes. Returns the previous value, or
+ * -1 for another value. */
 int rs_set_fft16_pass(int variant);
 int rs16_encode_dev(rs16_t *codec, uint8_t *const *d_shards, size_t n_shards, size_t len,
                     void *stream);

@@ -496,11 +496,142 @@ __global__ void __launch_bounds__(128, 4) fft16_pass16_kernel(const Fft16PassArg
   }
 }
 
+// Radix-2^V passes (V = 5 here; fft16_pass16_kernel is the V = 4 case written out) with
+// the runtime-constant networks: levels L .. L+V-1 of
+// one item's 2^V registers {i0 + q h : q < 2^V}, 2^(V-2) warps per CTA. The item's
+// registers are staged in shared memory (2^V x 2 KiB); the levels run in stages of two
+// (and one last single level for V = 5), each warp taking four registers per stage, and
+// the CTA exchanges through shared memory between stages; the last stage stores to the
+// destination. A two-level stage at relative level l takes registers base + j 2^l (j <
+// 4), base = warp w with two zero bits inserted at bit l; the single level 4 of V = 5
+// takes the pairs (2w, 2w + 16) and (2w + 1, 2w + 17). Inverse: stages by ascending
+// level; forward: the mirror image. The constant of level L+l for the block at register
+// i0 + q h is entry R - (R >> (L+l)) + ((grp >> L) << (V-1-l)) + (q >> (l+1)), as in the
+// radix-4 kernels. Each item reads and writes the scratch once for V levels.
+template <int V>
+struct Fft16Wide {
+  static constexpr int kWarps = 1 << (V - 2), kThreads = 32 * kWarps, kRegs = 1 << V;
+  static constexpr int kSmem = kRegs * 4 * 32 * 16;
+};
+
+template <int V>
+__global__ void __launch_bounds__(Fft16Wide<V>::kThreads, 8 / (1 << (V - 3)))
+    fft16_pass_wide_kernel(const Fft16PassArgs a) {
+  using Sh = Fft16Wide<V>;
+  extern __shared__ __align__(16) uint4 wstage[];  // [register][16-byte quarter][lane]
+  const uint32_t R = a.R, L = a.level, h = 1u << L;
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t chunks = (uint32_t)((a.G + 31) / 32), tasks = a.n_stripes * chunks;
+  const uint32_t items = (R >> V) * tasks;
+  auto cidx = [&](uint32_t l, uint32_t gb, uint32_t q) {
+    return R - (R >> (L + l)) + (gb << (V - 1 - l)) + (q >> (l + 1));
+  };
+  auto slot = [&](uint32_t q, uint32_t c) -> uint4 & { return wstage[(q * 4 + c) * 32 + lane]; };
+  auto load4 = [&](Reg16 (&r)[4], const uint32_t (&q)[4]) {
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const uint4 v = slot(q[j], c);
+        r[j][4 * c] = v.x, r[j][4 * c + 1] = v.y, r[j][4 * c + 2] = v.z, r[j][4 * c + 3] = v.w;
+      }
+  };
+  auto save4 = [&](const Reg16 (&r)[4], const uint32_t (&q)[4]) {
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) slot(q[j], c) = make_uint4(r[j][4 * c], r[j][4 * c + 1], r[j][4 * c + 2], r[j][4 * c + 3]);
+  };
+  // The registers and constants of this warp in stage t (in inverse order: t = 0 the
+  // levels 0, 1; t = 1 the levels 2, 3; t = 2 the level 4 of V = 5).
+  struct Stage {
+    uint32_t q[4];
+    uint32_t k[3];
+  };
+  auto stage_of = [&](int t, uint32_t gb) {
+    Stage st;
+    if (t < 2) {
+      const uint32_t l = 2 * t, base = (w & ((1u << l) - 1)) | ((w >> l) << (l + 2));
+#pragma unroll
+      for (int j = 0; j < 4; j++) st.q[j] = base + ((uint32_t)j << l);
+      st.k[0] = const_factors(a.cols, cidx(l, gb, base));
+      st.k[1] = const_factors(a.cols, cidx(l, gb, base + (2u << l)));
+      st.k[2] = const_factors(a.cols, cidx(l + 1, gb, base));
+    } else {
+      st.q[0] = 2 * w, st.q[1] = 2 * w + 16, st.q[2] = 2 * w + 1, st.q[3] = 2 * w + 17;
+      st.k[0] = st.k[1] = st.k[2] = const_factors(a.cols, cidx(4, gb, 2 * w));
+    }
+    return st;
+  };
+  auto run = [&](int t, Reg16 (&r)[4], const Stage &st) {
+    if (t == 2) {
+      bfly16_rt(r[0], r[1], st.k[0], a.inverse != 0);
+      bfly16_rt(r[2], r[3], st.k[0], a.inverse != 0);
+    } else if (a.inverse) {
+      bfly16_rt(r[0], r[1], st.k[0], true);
+      bfly16_rt(r[2], r[3], st.k[1], true);
+      bfly16_rt(r[0], r[2], st.k[2], true);
+      bfly16_rt(r[1], r[3], st.k[2], true);
+    } else {
+      bfly16_rt(r[0], r[2], st.k[2], false);
+      bfly16_rt(r[1], r[3], st.k[2], false);
+      bfly16_rt(r[0], r[1], st.k[0], false);
+      bfly16_rt(r[2], r[3], st.k[1], false);
+    }
+  };
+  constexpr int NS = V == 5 ? 3 : 2;
+  for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
+    const uint32_t grp = item / tasks, task = item - grp * tasks;
+    const uint32_t s = task / chunks;
+    const uint64_t gbase = (uint64_t)(task - s * chunks) * 32;
+    const uint32_t gb = grp >> L, i0 = gb * (h << V) + (grp & (h - 1));
+    const uint64_t rstride = (uint64_t)h * a.G * 16;  // words between the item's registers
+    const uint32_t *sbase = a.src + ((uint64_t)s * a.src_regs + a.src_start + i0) * a.G * 16;
+#pragma unroll
+    for (int i = 0; i < Sh::kRegs * 4 * 32 / Sh::kThreads; i++) {
+      const uint32_t idx = threadIdx.x + (uint32_t)Sh::kThreads * i;
+      const uint32_t ln = idx & 31u, c = (idx >> 5) & 3u, q = idx >> 7;
+      const uint64_t g = gbase + ln;
+      if (g < a.G) cp_async16(&wstage[idx], quarter16(sbase + q * rstride, a.G, g, c));
+    }
+    cp_async_commit();
+    Stage st = stage_of(a.inverse ? 0 : NS - 1, gb);  // constants load while the copies land
+    cp_async_wait_all();
+    __syncthreads();
+    Reg16 r[4];
+#pragma unroll
+    for (int n = 0; n < NS; n++) {
+      const int t = a.inverse ? n : NS - 1 - n;
+      if (n > 0) st = stage_of(t, gb);
+      load4(r, st.q);
+      if (n + 1 < NS) {
+        run(t, r, st);
+        save4(r, st.q);
+        __syncthreads();
+      }
+    }
+    __syncthreads();  // every warp has read its last stage: the next item may overwrite it
+    {
+      const int t = a.inverse ? NS - 1 : 0;
+      run(t, r, st);
+      const uint64_t g = gbase + lane;
+      if (g < a.G) {
+        const uint64_t db = (uint64_t)s * a.dst_regs + a.dst_start + i0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) store_reg16(a.dst + (db + (uint64_t)st.q[j] * h) * a.G * 16, a.G, g, r[j]);
+      }
+    }
+  }
+}
+
 // Which pass kernels run (rs_set_fft16_pass): 2 (default) the runtime-constant networks
-// with radix-16 passes where four levels remain, then radix-4 and radix-2; 1 the same
-// networks in radix-4 passes only; 0 the mask tables. The scaling, glue and store kernels
-// take the runtime-constant networks for 1 and 2. Measured on B200 (2 KiB shards): 2
-// against 1, (1024,1024) x 64 stripes 411 -> 463 GB/s, (4096,12288) x 2 240 -> 312 GB/s.
+// in passes of four levels (radix 16 through shared memory), of five for one pass when
+// the level count is odd, then of two; 1 radix-4 passes (and an odd top level alone)
+// only; 0 the mask tables. The scaling, glue and store kernels take the runtime-constant
+// networks for 1 and 2. Measured on B200 (2 KiB shards), 2 against 1: (1024,1024) x 64
+// stripes 411 -> 463 GB/s, (4096,12288) x 2 240 -> 312 GB/s; the five-level pass for odd
+// counts against a four-level and a one-level pass: (512,512) 476 -> 498 GB/s,
+// (2048,2048) 371 -> 387 GB/s (at (1024,1024), 5 + 5 levels ran 2% slower than 4 + 4 + 2).
 inline int &fft16_pass_variant() {
   static int v = 2;
   return v;
@@ -508,12 +639,13 @@ inline int &fft16_pass_variant() {
 inline bool fft16_rt() { return fft16_pass_variant() >= 1; }
 
 // The passes of a transform of 2^lg registers, in launch order: (lowest level, levels).
-// Inverse: levels ascending, four at a time when radix-16 passes run, then two, then an
-// odd top level alone; forward: the same passes in reverse order.
+// Inverse: levels ascending; forward: the same passes in reverse order.
 inline int fft16_passes(int lg, bool inverse, int (*out)[2]) {
   int n = 0, L = 0;
-  if (fft16_pass_variant() == 2)
+  if (fft16_pass_variant() == 2) {
+    if (lg >= 5 && lg % 2 == 1) out[n][0] = L, out[n++][1] = 5, L = 5;
     for (; L + 3 < lg; L += 4) out[n][0] = L, out[n++][1] = 4;
+  }
   for (; L + 1 < lg; L += 2) out[n][0] = L, out[n++][1] = 2;
   if (L < lg) out[n][0] = L, out[n++][1] = 1;
   if (!inverse)
@@ -526,9 +658,17 @@ inline int fft16_passes(int lg, bool inverse, int (*out)[2]) {
 inline cudaError_t launch_fft16_pass(const Fft16PassArgs &a, int lv, cudaStream_t st) {
   const uint64_t tasks = (uint64_t)a.n_stripes * ((a.G + 31) / 32), items = ((uint64_t)a.R >> lv) * tasks;
   if (items >= (1ull << 32)) return cudaErrorInvalidValue;
-  if (lv == 4) {  // four 128-thread CTAs per SM (registers)
-    const unsigned g4 = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)sm_count() * 4));
-    fft16_pass16_kernel<<<g4, 128, 0, st>>>(a);
+  if (lv == 4 || lv == 5) {  // 512 threads per SM (registers): 4 CTAs of 128 or 2 of 256
+    const int ctas = lv == 4 ? 4 : 2;
+    const unsigned gw = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)sm_count() * ctas));
+    if (lv == 4) {
+      fft16_pass16_kernel<<<gw, 128, 0, st>>>(a);
+    } else {
+      auto kern = fft16_pass_wide_kernel<5>;
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Fft16Wide<5>::kSmem);
+      if (e != cudaSuccess) return e;
+      kern<<<gw, Fft16Wide<5>::kThreads, Fft16Wide<5>::kSmem, st>>>(a);
+    }
     return cudaGetLastError();
   }
   const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)sm_count() * 16));

@@ -303,9 +303,10 @@ def test_decode_route_choice(gpu, O):
 @pytest.mark.parametrize("variant", [0, 1, 2])
 def test_both_pass_kernels_match_the_oracle(gpu, O, variant):
     """The tower FFT pass kernel with constants through shared-memory masks (0), through
-    compiled networks selected by the warp-uniform constant (1), and the latter with
-    radix-16 passes (2: four levels per pass where four remain, then radix-4 and radix-2
-    tails): the oracle's bytes on shapes with one and several cosets."""
+    compiled networks selected by the warp-uniform constant (1), and the latter in
+    passes of four levels through shared memory, of five for one pass when the level
+    count is odd (2; 32 and 128 registers: one five-level pass, 512: five and four): the
+    oracle's bytes on shapes with one and several cosets."""
     L = gpu.load()
     old = L.rs_set_fft16_pass(variant)
     try:
@@ -333,13 +334,14 @@ def test_both_pass_kernels_match_the_oracle(gpu, O, variant):
 
 def test_pass_kernel_variants_agree_on_large_batches(gpu, O):
     """Launches with several items per CTA and more items than one grid stride: pass
-    variants 0, 1 and 2 give the same bytes, and stripe 0 equals the oracle."""
+    variants 0, 1 and 2 give the same bytes, and stripe 0 equals the oracle (odd and
+    even level counts: 512 and 1024 registers)."""
     import torch
 
     L = gpu.load()
     old = L.rs_set_fft16_pass(1)
     try:
-        for k, m, S, stripes in [(256, 256, 8192, 17), (1000, 24, 4098, 5)]:
+        for k, m, S, stripes in [(256, 256, 8192, 17), (1000, 24, 4098, 5), (500, 40, 4098, 9)]:
             rs = gpu.ReedSolomon16(k, m)
             rs.set_route("fft")
             g = torch.Generator(device="cuda").manual_seed(k)
@@ -351,7 +353,7 @@ def test_pass_kernel_variants_agree_on_large_batches(gpu, O):
                 rs.encode_batch_dev(d, p, S, stripes)
                 torch.cuda.synchronize()
                 outs.append(p)
-            assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2]), (k, m)
+            assert all(torch.equal(outs[0], o) for o in outs[1:]), (k, m)
             host = d[0].cpu().numpy()
             assert np.array_equal(outs[1][0].cpu().numpy(), O.encode16(k, m, host)), (k, m)
     finally:
