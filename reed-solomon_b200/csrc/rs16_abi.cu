@@ -167,6 +167,9 @@ struct rs16_decoder {
   std::shared_ptr<const Gen16> gen;
   std::shared_ptr<const Plan> plan;
   std::shared_ptr<Exec> exec;
+  // k + m <= 256 on the automatic route: the GF(2^8) codec's prepared decoder of the same
+  // pattern, which rebuilds the shards once the tower's checks have passed.
+  std::shared_ptr<rs8_dec_t> sub;
 };
 
 namespace rsb {
@@ -281,7 +284,8 @@ static int fft16_reconstruct(const Gen16 &g, const Plan &plan, Exec &ex, uint8_t
 
 static int reconstruct16(const Gen16 &g, PlanCache *cache, const Plan *fixed, Exec &ex, int route,
                          uint8_t *const *shards, const size_t *lens, const uint8_t *present,
-                         size_t n_shards, bool data_only, bool dev, cudaStream_t st, rs8_t *sub = nullptr) {
+                         size_t n_shards, bool data_only, bool dev, cudaStream_t st, rs8_t *sub = nullptr,
+                         rs8_dec_t *sub_dec = nullptr) {
   size_t n = g.k + g.m;
   if (!shards || !lens || !present) return RS_ERR_INVALID_ARGUMENT;
   if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
@@ -296,6 +300,10 @@ static int reconstruct16(const Gen16 &g, PlanCache *cache, const Plan *fixed, Ex
     RSB_TRY(check_absent_buffers(lens, present, n, g.k, len, data_only));
     return dev ? rs8_reconstruct_dev(sub, shards, lens, present, n, data_only ? 1 : 0, st)
                : rs8_reconstruct(sub, shards, lens, present, n, data_only ? 1 : 0);
+  }
+  if (sub_dec && fixed && !dev) {  // a prepared decoder on the subfield codec
+    RSB_TRY(check_absent_buffers(lens, present, n, g.k, len, data_only));
+    return rs8_dec_reconstruct(sub_dec, shards, lens, present, n, data_only ? 1 : 0);
   }
   std::shared_ptr<const Plan> hold;
   const Plan *plan = fixed;
@@ -566,11 +574,18 @@ int rs16_prepare_decode(rs16_t *c, const uint8_t *present, size_t n_present, rs1
   if (count < g.k) return RS_TOO_FEW_SHARDS_PRESENT;
   std::shared_ptr<const Plan> plan;
   RSB_TRY(plan16_for(g, *c->plans, pres, plan, c->route.load()));
+  std::shared_ptr<rs8_dec_t> sub_dec;
+  if (rs8_t *sub = subfield(c)) {
+    rs8_dec_t *d8 = nullptr;
+    RSB_TRY(rs8_prepare_decode(sub, present, n, &d8));
+    sub_dec.reset(d8, rs8_dec_free);
+  }
   auto d = new (std::nothrow) rs16_decoder();
   if (!d) return RS_ERR_ALLOC;
   d->gen = c->gen;
   d->plan = plan;
   d->exec = c->exec;
+  d->sub = sub_dec;
   *out = d;
   return RS_OK;
 }
@@ -579,7 +594,7 @@ int rs16_dec_reconstruct(rs16_dec_t *d, uint8_t *const *shards, const size_t *le
                          size_t n_shards, int data_only) {
   if (!d) return RS_ERR_INVALID_ARGUMENT;
   return reconstruct16(*d->gen, nullptr, d->plan.get(), *d->exec, 0, shards, lens, present, n_shards,
-                       data_only != 0, false, nullptr);
+                       data_only != 0, false, nullptr, nullptr, d->sub.get());
 }
 
 int rs16_dec_clone(const rs16_dec_t *d, rs16_dec_t **out) {

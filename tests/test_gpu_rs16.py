@@ -94,9 +94,13 @@ def test_reconstruct_patterns(gpu, O, k, m, route):
                 assert np.array_equal(np.array(shards), full), (k, m, length, erased)
 
 
-def test_prepared_and_data_only(gpu, O):
+@pytest.mark.parametrize("route", ["auto", "matrix"])
+def test_prepared_and_data_only(gpu, O, route):
+    """Prepared decoders; with k + m <= 256 the automatic route rebuilds on the GF(2^8)
+    codec's prepared decoder after the tower's checks, the matrix route on the tower's."""
     k, m, length = 17, 33, 200
     rs = gpu.ReedSolomon16(k, m)
+    rs.set_route(route)
     data = rand(k, length, 1)
     full = np.concatenate([data, O.encode16(k, m, data)])
     erased = {1, 3, 20, 40}
@@ -112,6 +116,7 @@ def test_prepared_and_data_only(gpu, O):
     assert e.value.name == "InvalidShardFlags"
     k, m = 6, 4
     rs = gpu.ReedSolomon16(k, m)
+    rs.set_route(route)
     data = rand(k, 128, 2)
     full = np.concatenate([data, O.encode16(k, m, data)])
     erased = {2, k + 1}
