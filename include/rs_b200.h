@@ -539,6 +539,11 @@ int rs_fft_variant_count(void);
  * lanes per 32-column group, fewer registers per lane), -1 = automatic (as above).
  * Returns the previous value, or -1 when (k,k) has no FFT kernel. */
 int rs_set_fft_lanes(size_t k, int wide);
+/* Tuning hook, no counterpart in the reference: host threads (1..64, default 8) that
+ * gather a host-pointer stripe into pinned memory and scatter its parity back, for
+ * stripes with at least 8 MiB to move. Returns the previous value; other values leave
+ * it unchanged. */
+int rs_set_host_copy_threads(int n);
 /* Tuning hook: tile shape of the matrix kernel for batched and single calls
  * (parity rows per thread x output rows per CTA), 0..rs_matrix_variant_count()-1. */
 int rs_set_matrix_variant(int variant);

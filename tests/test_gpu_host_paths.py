@@ -85,13 +85,16 @@ def test_host_batch_strided_stripes(gpu, O):
 
 
 @pytest.mark.parametrize("pinned", [False, True])
-def test_single_stripe_host_encode_in_column_chunks(gpu, O, pinned):
-    """One RS(32,32) stripe of 1 MiB + 333-byte shards, separately allocated (the
-    reference's Vec<u8> shards): 32 MiB of data, cut into column chunks on the device
-    with a ragged last chunk."""
+@pytest.mark.parametrize("length", [(1 << 20) + 333, (4 << 20) + 333])
+def test_single_stripe_host_encode_in_column_chunks(gpu, O, pinned, length):
+    """One RS(32,32) stripe of separately allocated shards (the reference's Vec<u8>
+    shards): at 1 MiB + 333 bytes the stripe is gathered into pinned memory by host
+    threads in 1 MiB pieces (a ragged last piece per shard); at 4 MiB + 333 bytes (more
+    than 256 MiB of shards) it goes through the column-chunk pipeline, with a ragged
+    last chunk."""
     import torch
 
-    k, m, length = 32, 32, (1 << 20) + 333
+    k, m = 32, 32
     rng = np.random.default_rng(35 + pinned)
     shards = []
     for i in range(k + m):
