@@ -151,6 +151,11 @@ int launch_gf8(const ApplyArgs &a, const PtrTable *pt, bool verify, cudaStream_t
 // length (a packed odd length would put most rows on the byte paths).
 static size_t pitch16(size_t len) { return (len + 15) & ~size_t(15); }
 
+// Host-pointer encodes and reconstructs of stripes up to this size (the rows crossing
+// the link) go through pinned staging in one piece; larger encodes through the
+// column-chunk pipeline, larger reconstructs through per-shard copies.
+static constexpr size_t kStagedStripeBytes = 256u << 20;
+
 // Encode route for a shape and length: the compiled kernel where the shape has one and
 // the shard holds at least two 32-column groups, else the matrix kernel. Row alignment
 // does not change the route: with the aligned-window staging of unaligned rows the
@@ -314,13 +319,34 @@ static int reconstruct8(const Gen8 &g, PlanCache *cache, const Plan *fixed, Exec
   RSB_CU(cudaSetDevice(g.device));
   const size_t pitch = pitch16(len);
   RSB_TRY(ex.buf.ensure((g.k + rows) * pitch));
-  for (size_t t = 0; t < g.k; t++)
-    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + t * pitch, shards[plan->survivors[t]], len,
-                           cudaMemcpyHostToDevice, ex.stream));
   a.in_base = ex.buf.ptr;
   a.in_row_stride = pitch;
   a.out_base = ex.buf.ptr + g.k * pitch;
   a.out_row_stride = pitch;
+  if ((g.k + rows) * pitch <= kStagedStripeBytes) {
+    // As rs8_encode: survivors gathered into pinned memory by host threads, one copy each
+    // way, the rebuilt rows scattered back.
+    RSB_TRY(ex.io.ensure((g.k + rows) * pitch));
+    uint8_t *h = ex.io.ptr;
+    const size_t piece = std::min<size_t>(len, 1u << 20), per = (len + piece - 1) / piece;
+    host_copy_pieces(g.k * per, g.k * len, [&](size_t i) {
+      const size_t t = i / per, off = (i % per) * piece;
+      memcpy(h + t * pitch + off, shards[plan->survivors[t]] + off, std::min(piece, len - off));
+    });
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr, h, g.k * pitch, cudaMemcpyHostToDevice, ex.stream));
+    RSB_TRY(launch_gf8(a, nullptr, false, ex.stream));
+    RSB_CU(cudaMemcpyAsync(h + g.k * pitch, ex.buf.ptr + g.k * pitch, rows * pitch, cudaMemcpyDeviceToHost,
+                           ex.stream));
+    RSB_CU(cudaStreamSynchronize(ex.stream));
+    host_copy_pieces(rows * per, rows * len, [&](size_t i) {
+      const size_t j = i / per, off = (i % per) * piece;
+      memcpy(shards[outs[j]] + off, h + (g.k + j) * pitch + off, std::min(piece, len - off));
+    });
+    return RS_OK;
+  }
+  for (size_t t = 0; t < g.k; t++)
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + t * pitch, shards[plan->survivors[t]], len,
+                           cudaMemcpyHostToDevice, ex.stream));
   RSB_TRY(launch_gf8(a, nullptr, false, ex.stream));
   for (size_t j = 0; j < rows; j++)
     RSB_CU(cudaMemcpyAsync(shards[outs[j]], ex.buf.ptr + (g.k + j) * pitch, len,
@@ -559,9 +585,6 @@ int rs8_set_route(rs8_t *c, int route) {
 // only when it has finished: the next chunk's copy-in (another copy engine) and kernel
 // then run while it waits. Pinned shards make every copy asynchronous.
 static constexpr size_t kChunkStripeBytes = 8u << 20;  // data bytes per chunk (all shards)
-// Host-pointer encodes of stripes up to this size (all shards) go through pinned staging
-// in one piece; larger ones through the column-chunk pipeline.
-static constexpr size_t kStagedStripeBytes = 256u << 20;
 
 static int encode8_host_chunked(rs8_t *c, uint8_t *const *shards, size_t len) {
   const Gen8 &g = *c->gen;
