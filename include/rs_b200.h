@@ -544,6 +544,11 @@ int rs_set_fft_lanes(size_t k, int wide);
  * stripes with at least 8 MiB to move. Returns the previous value; other values leave
  * it unchanged. */
 int rs_set_host_copy_threads(int n);
+/* Tuning hook, no counterpart in the reference: host-pointer encodes and reconstructs
+ * gather their rows into pinned memory and cross the link in one copy each way (1, the
+ * default, up to 256 MiB per call) or copy each shard on its own (0). Same bytes.
+ * Returns the previous value. */
+int rs_set_host_staging(int on);
 /* Tuning hook: tile shape of the matrix kernel for batched and single calls
  * (parity rows per thread x output rows per CTA), 0..rs_matrix_variant_count()-1. */
 int rs_set_matrix_variant(int variant);

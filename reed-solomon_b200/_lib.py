@@ -28,6 +28,7 @@ SIGNATURES = {
     "rs_fft_variant_count": (_int, []),
     "rs_set_fft_lanes": (_int, [_sz, _int]),
     "rs_set_host_copy_threads": (_int, [_int]),
+    "rs_set_host_staging": (_int, [_int]),
     "rs_set_matrix_variant": (_int, [_int]),
     "rs_set_fft16_pass": (_int, [_int]),
     "rs_set_matrix_bits": (_int, [_int]),

@@ -271,11 +271,33 @@ static int fft16_reconstruct(const Gen16 &g, const Plan &plan, Exec &ex, uint8_t
   RSB_TRY(ex.aux.ensure(tbytes + sbytes));
   std::vector<uint8_t *> ptrs(n);
   for (size_t i = 0; i < n; i++) ptrs[i] = ex.buf.ptr + i * len;
-  for (uint32_t s : plan.survivors)
-    RSB_CU(cudaMemcpyAsync(ptrs[s], shards[s], len, cudaMemcpyHostToDevice, ex.stream));
+  // Staged (as rs16_encode): the present rows gathered into pinned memory in their slots
+  // of the n-row layout, which crosses the link in one copy each way.
+  const bool staged = host_staged(n * len);
+  if (staged) {
+    RSB_TRY(ex.io.ensure(n * len));
+    uint8_t *h = ex.io.ptr;
+    const std::vector<uint32_t> &sv = plan.survivors;
+    gather_rows(h, len, sv.size(), len, [&](size_t i) { return shards[sv[i]]; });
+    // gather_rows packed them; move each to its slot, last first (a slot index is at
+    // least its survivor position, so no row is overwritten before it moves).
+    for (size_t i = sv.size(); i-- > 0;)
+      if (sv[i] != i) memmove(h + (size_t)sv[i] * len, h + i * len, len);
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr, h, n * len, cudaMemcpyHostToDevice, ex.stream));
+  } else {
+    for (uint32_t s : plan.survivors)
+      RSB_CU(cudaMemcpyAsync(ptrs[s], shards[s], len, cudaMemcpyHostToDevice, ex.stream));
+  }
   RSB_CU(cudaMemcpyAsync(ex.aux.ptr, ptrs.data(), n * sizeof(void *), cudaMemcpyHostToDevice, ex.stream));
   RSB_TRY(fft16_decode_run(d, d_cols, ex.aux.ptr + tbytes, sbytes, reinterpret_cast<uint8_t *const *>(ex.aux.ptr),
                            d_targets, rows, len, ex.stream));
+  if (staged) {
+    RSB_CU(cudaMemcpyAsync(ex.io.ptr, ex.buf.ptr, n * len, cudaMemcpyDeviceToHost, ex.stream));
+    RSB_CU(cudaStreamSynchronize(ex.stream));
+    const uint8_t *h = ex.io.ptr;
+    for (size_t j = 0; j < rows; j++) memcpy(shards[d.targets[j]], h + (size_t)d.targets[j] * len, len);
+    return RS_OK;
+  }
   for (size_t j = 0; j < rows; j++)
     RSB_CU(cudaMemcpyAsync(shards[d.targets[j]], ptrs[d.targets[j]], len, cudaMemcpyDeviceToHost, ex.stream));
   RSB_CU(cudaStreamSynchronize(ex.stream));
@@ -329,9 +351,16 @@ static int reconstruct16(const Gen16 &g, PlanCache *cache, const Plan *fixed, Ex
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
   RSB_TRY(ex.buf.ensure((g.k + rows) * len));
-  for (size_t t = 0; t < g.k; t++)
-    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + t * len, shards[plan->survivors[t]], len, cudaMemcpyHostToDevice,
-                           ex.stream));
+  const bool staged = host_staged((g.k + rows) * len);  // as rs16_encode
+  if (staged) {
+    RSB_TRY(ex.io.ensure((g.k + rows) * len));
+    gather_rows(ex.io.ptr, len, g.k, len, [&](size_t t) { return shards[plan->survivors[t]]; });
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr, ex.io.ptr, g.k * len, cudaMemcpyHostToDevice, ex.stream));
+  } else {
+    for (size_t t = 0; t < g.k; t++)
+      RSB_CU(cudaMemcpyAsync(ex.buf.ptr + t * len, shards[plan->survivors[t]], len, cudaMemcpyHostToDevice,
+                             ex.stream));
+  }
   Apply16Args a{};
   a.in_base = ex.buf.ptr;
   a.in_row_stride = len;
@@ -343,6 +372,13 @@ static int reconstruct16(const Gen16 &g, PlanCache *cache, const Plan *fixed, Ex
   a.n_sym = len / 2;
   a.n_stripes = 1;
   RSB_TRY(launch_gf16(a, false, ex.stream));
+  if (staged) {
+    RSB_CU(cudaMemcpyAsync(ex.io.ptr + g.k * len, ex.buf.ptr + g.k * len, rows * len, cudaMemcpyDeviceToHost,
+                           ex.stream));
+    RSB_CU(cudaStreamSynchronize(ex.stream));
+    scatter_rows(ex.io.ptr + g.k * len, len, rows, len, [&](size_t j) { return shards[outs[j]]; });
+    return RS_OK;
+  }
   for (size_t j = 0; j < rows; j++)
     RSB_CU(cudaMemcpyAsync(shards[outs[j]], ex.buf.ptr + (g.k + j) * len, len, cudaMemcpyDeviceToHost,
                            ex.stream));
@@ -456,12 +492,24 @@ int rs16_encode(rs16_t *c, uint8_t *const *shards, size_t n_shards, size_t len) 
   if (n_shards != n) return n_shards < n ? RS_TOO_FEW_SHARDS : RS_TOO_MANY_SHARDS;
   RSB_TRY(check_len16(len));
   if (subfield_encode(c, len, 1)) return rs8_encode(c->sub, shards, n_shards, len);
+  for (size_t i = 0; i < n; i++)
+    if (!shards[i]) return RS_ERR_INVALID_ARGUMENT;
   Exec &ex = *c->exec;
   std::lock_guard<std::mutex> lock(ex.mu);
   RSB_CU(cudaSetDevice(g.device));
   RSB_TRY(ex.buf.ensure(n * len));
-  for (size_t i = 0; i < g.k; i++)
-    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * len, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
+  // Up to kStagedCallBytes (host_staged) the data rows are gathered into pinned memory
+  // and cross the link in one copy (a tower stripe can hold thousands of shards: one
+  // pageable copy each costs microseconds apiece); the parity comes back the same way.
+  const bool staged = host_staged(n * len);
+  if (staged) {
+    RSB_TRY(ex.io.ensure(n * len));
+    gather_rows(ex.io.ptr, len, g.k, len, [&](size_t i) { return shards[i]; });
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr, ex.io.ptr, g.k * len, cudaMemcpyHostToDevice, ex.stream));
+  } else {
+    for (size_t i = 0; i < g.k; i++)
+      RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * len, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
+  }
   if (use_fft16(c, len)) {
     RSB_TRY(fft16_encode(g, ex.buf.ptr, len, 0, ex.buf.ptr + g.k * len, len, 0, 1, len, nullptr, ex.stream));
   } else {
@@ -476,6 +524,13 @@ int rs16_encode(rs16_t *c, uint8_t *const *shards, size_t n_shards, size_t len) 
     a.n_sym = len / 2;
     a.n_stripes = 1;
     RSB_TRY(launch_gf16(a, false, ex.stream));
+  }
+  if (staged) {
+    RSB_CU(cudaMemcpyAsync(ex.io.ptr + g.k * len, ex.buf.ptr + g.k * len, g.m * len, cudaMemcpyDeviceToHost,
+                           ex.stream));
+    RSB_CU(cudaStreamSynchronize(ex.stream));
+    scatter_rows(ex.io.ptr + g.k * len, len, g.m, len, [&](size_t j) { return shards[g.k + j]; });
+    return RS_OK;
   }
   for (size_t j = 0; j < g.m; j++)
     RSB_CU(cudaMemcpyAsync(shards[g.k + j], ex.buf.ptr + (g.k + j) * len, len, cudaMemcpyDeviceToHost,

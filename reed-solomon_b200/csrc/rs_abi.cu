@@ -151,10 +151,6 @@ int launch_gf8(const ApplyArgs &a, const PtrTable *pt, bool verify, cudaStream_t
 // length (a packed odd length would put most rows on the byte paths).
 static size_t pitch16(size_t len) { return (len + 15) & ~size_t(15); }
 
-// Host-pointer encodes and reconstructs of stripes up to this size (the rows crossing
-// the link) go through pinned staging in one piece; larger encodes through the
-// column-chunk pipeline, larger reconstructs through per-shard copies.
-static constexpr size_t kStagedStripeBytes = 256u << 20;
 
 // Encode route for a shape and length: the compiled kernel where the shape has one and
 // the shard holds at least two 32-column groups, else the matrix kernel. Row alignment
@@ -323,25 +319,18 @@ static int reconstruct8(const Gen8 &g, PlanCache *cache, const Plan *fixed, Exec
   a.in_row_stride = pitch;
   a.out_base = ex.buf.ptr + g.k * pitch;
   a.out_row_stride = pitch;
-  if ((g.k + rows) * pitch <= kStagedStripeBytes) {
+  if (host_staged((g.k + rows) * pitch)) {
     // As rs8_encode: survivors gathered into pinned memory by host threads, one copy each
     // way, the rebuilt rows scattered back.
     RSB_TRY(ex.io.ensure((g.k + rows) * pitch));
     uint8_t *h = ex.io.ptr;
-    const size_t piece = std::min<size_t>(len, 1u << 20), per = (len + piece - 1) / piece;
-    host_copy_pieces(g.k * per, g.k * len, [&](size_t i) {
-      const size_t t = i / per, off = (i % per) * piece;
-      memcpy(h + t * pitch + off, shards[plan->survivors[t]] + off, std::min(piece, len - off));
-    });
+    gather_rows(h, pitch, g.k, len, [&](size_t t) { return shards[plan->survivors[t]]; });
     RSB_CU(cudaMemcpyAsync(ex.buf.ptr, h, g.k * pitch, cudaMemcpyHostToDevice, ex.stream));
     RSB_TRY(launch_gf8(a, nullptr, false, ex.stream));
     RSB_CU(cudaMemcpyAsync(h + g.k * pitch, ex.buf.ptr + g.k * pitch, rows * pitch, cudaMemcpyDeviceToHost,
                            ex.stream));
     RSB_CU(cudaStreamSynchronize(ex.stream));
-    host_copy_pieces(rows * per, rows * len, [&](size_t i) {
-      const size_t j = i / per, off = (i % per) * piece;
-      memcpy(shards[outs[j]] + off, h + (g.k + j) * pitch + off, std::min(piece, len - off));
-    });
+    scatter_rows(h + g.k * pitch, pitch, rows, len, [&](size_t j) { return shards[outs[j]]; });
     return RS_OK;
   }
   for (size_t t = 0; t < g.k; t++)
@@ -447,6 +436,10 @@ int rs_set_fft_lanes(size_t k, int wide) {
   c = wide < 0 ? kFftLanesDefault[log2_index(k)] : wide;
   fft_shape_auto((int)k) = wide < 0;
   return old;
+}
+
+int rs_set_host_staging(int on) {
+  return host_staging_on().exchange(on ? 1 : 0);
 }
 
 int rs_set_host_copy_threads(int n) {
@@ -631,28 +624,20 @@ int rs8_encode(rs8_t *c, uint8_t *const *shards, size_t n_shards, size_t len) {
   for (size_t i = 0; i < n; i++)
     if (!shards[i]) return RS_ERR_INVALID_ARGUMENT;
   const size_t pitch = pitch16(len);
-  if (n * pitch > kStagedStripeBytes) return encode8_host_chunked(c, shards, len);
+  if (!host_staged(n * pitch)) return encode8_host_chunked(c, shards, len);
   // The shards are gathered into pinned memory by host threads and cross the link as one
   // copy each way: pageable copies of separate shards ran at 8-23 GB/s host to device and
   // 3-13 GB/s back on B200 hosts, against ~55 GB/s pinned.
   RSB_TRY(ex.buf.ensure(n * pitch));
   RSB_TRY(ex.io.ensure(n * pitch));
   uint8_t *h = ex.io.ptr;
-  const size_t piece = std::min<size_t>(len, 1u << 20), per = (len + piece - 1) / piece;
-  auto copy = [&](size_t i, bool in) {
-    const size_t row = i / per, off = (i % per) * piece, w = std::min(piece, len - off);
-    if (in)
-      memcpy(h + row * pitch + off, shards[row] + off, w);
-    else
-      memcpy(shards[g.k + row] + off, h + (g.k + row) * pitch + off, w);
-  };
-  host_copy_pieces(g.k * per, g.k * len, [&](size_t i) { copy(i, true); });
+  gather_rows(h, pitch, g.k, len, [&](size_t i) { return shards[i]; });
   RSB_CU(cudaMemcpyAsync(ex.buf.ptr, h, g.k * pitch, cudaMemcpyHostToDevice, ex.stream));
   RSB_TRY(encode8_strided(c, ex.buf.ptr, pitch, 0, ex.buf.ptr + g.k * pitch, pitch, 0, 1, len, ex.stream));
   RSB_CU(cudaMemcpyAsync(h + g.k * pitch, ex.buf.ptr + g.k * pitch, g.m * pitch, cudaMemcpyDeviceToHost,
                          ex.stream));
   RSB_CU(cudaStreamSynchronize(ex.stream));
-  host_copy_pieces(g.m * per, g.m * len, [&](size_t i) { copy(i, false); });
+  scatter_rows(h + g.k * pitch, pitch, g.m, len, [&](size_t j) { return shards[g.k + j]; });
   return RS_OK;
 }
 

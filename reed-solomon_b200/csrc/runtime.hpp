@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <cstring>
 #include <memory>
 #include <mutex>
 #include <shared_mutex>
@@ -160,6 +161,38 @@ inline void host_copy_pieces(size_t count, size_t total_bytes, const F &copy_pie
   work();
   for (auto &t : ts) t.join();
 }
+
+// Rows of `len` bytes between host buffers and pinned staging `pitch` apart, by host
+// threads in pieces of at most 1 MiB: gather copies row i from src(i) to h + i * pitch,
+// scatter copies h + i * pitch to dst(i).
+template <class SrcF>
+inline void gather_rows(uint8_t *h, size_t pitch, size_t count, size_t len, const SrcF &src) {
+  const size_t piece = std::min<size_t>(len, 1u << 20), per = (len + piece - 1) / piece;
+  host_copy_pieces(count * per, count * len, [&](size_t i) {
+    const size_t r = i / per, off = (i % per) * piece;
+    memcpy(h + r * pitch + off, src(r) + off, std::min(piece, len - off));
+  });
+}
+template <class DstF>
+inline void scatter_rows(const uint8_t *h, size_t pitch, size_t count, size_t len, const DstF &dst) {
+  const size_t piece = std::min<size_t>(len, 1u << 20), per = (len + piece - 1) / piece;
+  host_copy_pieces(count * per, count * len, [&](size_t i) {
+    const size_t r = i / per, off = (i % per) * piece;
+    memcpy(dst(r) + off, h + r * pitch + off, std::min(piece, len - off));
+  });
+}
+
+// Host-pointer calls whose rows crossing the link stay within this size are staged
+// through pinned memory (PinnedBuf, gather_rows / scatter_rows) in one copy each way.
+constexpr size_t kStagedCallBytes = 256u << 20;
+
+// Whether host-pointer calls stage through pinned memory (rs_set_host_staging; on by
+// default), and whether a call moving `bytes` across the link does.
+inline std::atomic<int> &host_staging_on() {
+  static std::atomic<int> on{1};
+  return on;
+}
+inline bool host_staged(size_t bytes) { return host_staging_on().load() != 0 && bytes <= kStagedCallBytes; }
 
 // Serialises host-pointer calls on one codec and owns their staging memory.
 struct Exec {

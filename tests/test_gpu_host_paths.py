@@ -111,3 +111,42 @@ def test_single_stripe_host_encode_in_column_chunks(gpu, O, pinned, length):
     assert np.array_equal(parity, _device_parity(gpu, k, m, data[None])[0])
     _oracle_check(O, k, m, data, parity, rng)
     assert rs.verify(shards)
+
+
+@pytest.mark.parametrize("staging", [1, 0])
+def test_host_calls_with_and_without_pinned_staging(gpu, O, staging):
+    """Host-pointer encode and reconstruct of both coders, with the rows gathered into
+    pinned memory (1, the default) or copied shard by shard (0): the oracle's bytes.
+    Covers a tower shape with the FFT encode and decoder (k + m > 256) and one on the
+    tower matrix kernels."""
+    L = gpu.load()
+    old = L.rs_set_host_staging(staging)
+    try:
+        rng = np.random.default_rng(40 + staging)
+        for k, m, length in [(32, 32, 4096 + 3), (10, 4, 70000)]:
+            data = rng.integers(0, 256, size=(k, length), dtype=np.uint8)
+            full = np.concatenate([data, O.encode8(k, m, data)])
+            rs = gpu.ReedSolomon(k, m)
+            shards = [s.copy() for s in data] + [np.zeros(length, np.uint8) for _ in range(m)]
+            rs.encode(shards)
+            assert np.array_equal(np.array(shards), full), (k, m)
+            erased = set(rng.choice(k + m, size=m, replace=False).tolist())
+            for e in erased:
+                shards[e][:] = 0
+            rs.reconstruct([(s, i not in erased) for i, s in enumerate(shards)])
+            assert np.array_equal(np.array(shards), full), (k, m)
+        for k, m, length, route in [(300, 200, 66, "fft"), (20, 300, 130, "matrix")]:
+            data = rng.integers(0, 256, size=(k, length), dtype=np.uint8)
+            full = np.concatenate([data, O.encode16(k, m, data)])
+            rs = gpu.ReedSolomon16(k, m)
+            rs.set_route(route)
+            shards = [s.copy() for s in data] + [np.zeros(length, np.uint8) for _ in range(m)]
+            rs.encode(shards)
+            assert np.array_equal(np.array(shards), full), (k, m)
+            erased = set(rng.choice(k + m, size=m, replace=False).tolist())
+            for e in erased:
+                shards[e][:] = 0
+            rs.reconstruct([(s, i not in erased) for i, s in enumerate(shards)])
+            assert np.array_equal(np.array(shards), full), (k, m)
+    finally:
+        L.rs_set_host_staging(old)
