@@ -567,7 +567,15 @@ int rs16_verify(rs16_t *c, const uint8_t *const *shards, size_t n_shards, size_t
   RSB_TRY(ex.buf.ensure(n * len));
   RSB_TRY(ex.aux.ensure(64));
   for (size_t i = 0; i < n; i++)
-    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * len, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
+    if (!shards[i]) return RS_ERR_INVALID_ARGUMENT;
+  if (host_staged(n * len)) {  // as rs16_encode: one copy of the gathered stripe
+    RSB_TRY(ex.io.ensure(n * len));
+    gather_rows(ex.io.ptr, len, n, len, [&](size_t i) { return shards[i]; });
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr, ex.io.ptr, n * len, cudaMemcpyHostToDevice, ex.stream));
+  } else {
+    for (size_t i = 0; i < n; i++)
+      RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * len, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
+  }
   uint32_t *flag = reinterpret_cast<uint32_t *>(ex.aux.ptr);
   RSB_CU(cudaMemsetAsync(flag, 0, 4, ex.stream));
   Apply16Args a{};

@@ -743,7 +743,15 @@ int rs8_verify(rs8_t *c, const uint8_t *const *shards, size_t n_shards, size_t l
   RSB_TRY(ex.buf.ensure(n * pitch));
   RSB_TRY(ex.aux.ensure(64));
   for (size_t i = 0; i < n; i++)
-    RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * pitch, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
+    if (!shards[i]) return RS_ERR_INVALID_ARGUMENT;
+  if (host_staged(n * pitch)) {  // as rs8_encode: one copy of the gathered stripe
+    RSB_TRY(ex.io.ensure(n * pitch));
+    gather_rows(ex.io.ptr, pitch, n, len, [&](size_t i) { return shards[i]; });
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr, ex.io.ptr, n * pitch, cudaMemcpyHostToDevice, ex.stream));
+  } else {
+    for (size_t i = 0; i < n; i++)
+      RSB_CU(cudaMemcpyAsync(ex.buf.ptr + i * pitch, shards[i], len, cudaMemcpyHostToDevice, ex.stream));
+  }
   uint32_t *flag = reinterpret_cast<uint32_t *>(ex.aux.ptr);
   RSB_CU(cudaMemsetAsync(flag, 0, 4, ex.stream));
   ApplyArgs a{};
