@@ -443,8 +443,8 @@ int rs_set_host_staging(int on) {
 }
 
 int rs_set_host_copy_threads(int n) {
-  const int old = host_copy_threads();
-  if (n >= 1 && n <= 64) host_copy_threads() = n;
+  const int old = host_copy_threads().load();
+  if (n >= 1 && n <= 64) host_copy_threads().store(n);
   return old;
 }
 

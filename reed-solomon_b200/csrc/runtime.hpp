@@ -135,17 +135,18 @@ struct PinnedBuf {
   }
 };
 
-// Host copies of `count` pieces (copy_piece(i) for i < count), on up to MAXT host
-// threads (the caller's included) when there are at least 8 MiB to move, where one
-// thread's memcpy rate (about 11 GB/s on the B200 boxes' hosts) would bound the call.
-inline int &host_copy_threads() {
-  static int t = 8;
+// Host copies of `count` pieces (copy_piece(i) for i < count), on up to
+// host_copy_threads() host threads (the caller's included) when there are at least
+// 8 MiB to move, where one thread's memcpy rate (about 11 GB/s on the B200 boxes' hosts)
+// would bound the call. A thread that cannot be started leaves its share to the others.
+inline std::atomic<int> &host_copy_threads() {
+  static std::atomic<int> t{8};
   return t;
 }
 template <class F>
 inline void host_copy_pieces(size_t count, size_t total_bytes, const F &copy_piece) {
   const unsigned hw = std::thread::hardware_concurrency();
-  const size_t maxt = (size_t)std::max(1, host_copy_threads());
+  const size_t maxt = (size_t)std::max(1, host_copy_threads().load());
   size_t nt = total_bytes >= (8u << 20) ? std::min<size_t>(std::min<size_t>(maxt, hw ? hw : 1), count) : 1;
   if (nt <= 1) {
     for (size_t i = 0; i < count; i++) copy_piece(i);
@@ -156,8 +157,11 @@ inline void host_copy_pieces(size_t count, size_t total_bytes, const F &copy_pie
     for (size_t i = next.fetch_add(1); i < count; i = next.fetch_add(1)) copy_piece(i);
   };
   std::vector<std::thread> ts;
-  ts.reserve(nt - 1);
-  for (size_t t = 1; t < nt; t++) ts.emplace_back(work);
+  try {
+    ts.reserve(nt - 1);
+    for (size_t t = 1; t < nt; t++) ts.emplace_back(work);
+  } catch (...) {
+  }
   work();
   for (auto &t : ts) t.join();
 }
