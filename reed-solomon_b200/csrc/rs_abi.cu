@@ -671,6 +671,17 @@ int rs8_encode_rows(rs8_t *c, const uint8_t *data, size_t data_len, size_t row_l
   const size_t pitch = pitch16(row_len);
   RSB_TRY(ex.buf.ensure(n * pitch));
   uint8_t *d_par = ex.buf.ptr + g.k * pitch;
+  if (host_staged(n * pitch)) {  // as rs8_encode
+    RSB_TRY(ex.io.ensure(n * pitch));
+    uint8_t *h = ex.io.ptr;
+    gather_rows(h, pitch, g.k, row_len, [&](size_t i) { return data + i * row_len; });
+    RSB_CU(cudaMemcpyAsync(ex.buf.ptr, h, g.k * pitch, cudaMemcpyHostToDevice, ex.stream));
+    RSB_TRY(encode8_strided(c, ex.buf.ptr, pitch, 0, d_par, pitch, 0, 1, row_len, ex.stream));
+    RSB_CU(cudaMemcpyAsync(h + g.k * pitch, d_par, g.m * pitch, cudaMemcpyDeviceToHost, ex.stream));
+    RSB_CU(cudaStreamSynchronize(ex.stream));
+    scatter_rows(h + g.k * pitch, pitch, g.m, row_len, [&](size_t j) { return parity + j * row_len; });
+    return RS_OK;
+  }
   RSB_CU(cudaMemcpy2DAsync(ex.buf.ptr, pitch, data, row_len, row_len, g.k, cudaMemcpyHostToDevice, ex.stream));
   RSB_TRY(encode8_strided(c, ex.buf.ptr, pitch, 0, d_par, pitch, 0, 1, row_len, ex.stream));
   RSB_CU(cudaMemcpy2DAsync(parity, row_len, d_par, pitch, row_len, g.m, cudaMemcpyDeviceToHost, ex.stream));

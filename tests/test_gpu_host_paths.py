@@ -115,7 +115,8 @@ def test_single_stripe_host_encode_in_column_chunks(gpu, O, pinned, length):
 
 @pytest.mark.parametrize("staging", [1, 0])
 def test_host_calls_with_and_without_pinned_staging(gpu, O, staging):
-    """Host-pointer encode, verify and reconstruct of both coders, with the rows gathered into
+    """Host-pointer encode (and encode_rows), verify and reconstruct of both coders, with
+    the rows gathered into
     pinned memory (1, the default) or copied shard by shard (0): the oracle's bytes.
     Covers a tower shape with the FFT encode and decoder (k + m > 256) and one on the
     tower matrix kernels."""
@@ -130,6 +131,8 @@ def test_host_calls_with_and_without_pinned_staging(gpu, O, staging):
             shards = [s.copy() for s in data] + [np.zeros(length, np.uint8) for _ in range(m)]
             rs.encode(shards)
             assert np.array_equal(np.array(shards), full), (k, m)
+            rows = rs.encode_rows(np.ascontiguousarray(data).reshape(-1), length)
+            assert np.array_equal(np.asarray(rows).reshape(m, length), full[k:]), (k, m)
             assert rs.verify(shards)
             shards[k][-1] ^= 1
             assert not rs.verify(shards)
