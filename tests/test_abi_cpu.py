@@ -139,6 +139,14 @@ def test_fft_tuning_hooks_and_automatic_choice(rsb):
     assert L.rs_set_fft_lanes(128, -1) == wide
     assert L.rs_set_fft_lanes(128, 2) == -1
     assert L.rs_set_fft_lanes(14, 0) == -1
+    # Host-pointer staging switches (host state only).
+    t = L.rs_set_host_copy_threads(4)
+    assert t >= 1
+    assert L.rs_set_host_copy_threads(0) == 4  # out of range: unchanged
+    assert L.rs_set_host_copy_threads(t) == 4
+    on = L.rs_set_host_staging(0)
+    assert on == 1
+    assert L.rs_set_host_staging(1) == 0
 
 
 def test_tuning_configurations_match_the_tuner(rsb):
